@@ -1,0 +1,227 @@
+/*
+ * libttcuda -- C ABI of the B200 (sm_100a) tensor-train rounding engine.
+ *
+ * Every entry point replaces one method of the Julia package TensorTrains
+ * (rodrigofj99/Tensor-Train-Julia); the comment above each declaration names the
+ * reference method (file:line) whose meaning, argument order and error behaviour
+ * it keeps.  Host-side tensors use the reference's memory layout unchanged:
+ *   TTvector core k : column-major (n_k, r_{k-1}, r_k)            (src/tt_tools.jl:24-34)
+ *   TToperator core : column-major (n_k, n_k, R_{k-1}, R_k)       (src/tt_tools.jl:61-71)
+ * so a Julia `ccall` passes `pointer.(x.ttv_vec)` directly, with no host transposes.
+ * Ranks, dims and orthogonality flags are int64 like Julia's `Vector{Int64}`.
+ *
+ * All functions return a ttc_status; on failure ttc_last_error() holds a message.
+ * Output tensors are written into caller-allocated buffers whose capacities
+ * (rks_cap) the caller states; output ranks never exceed the capacities documented
+ * per function, and the written ranks are returned in `rks`.
+ */
+#ifndef TTCUDA_H
+#define TTCUDA_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  TTC_OK = 0,
+  TTC_EARG = 1,       /* invalid argument        -> Julia ArgumentError            */
+  TTC_EDIM = 2,       /* dimension mismatch      -> DimensionMismatch / @assert    */
+  TTC_ENOCONV = 3,    /* Jacobi SVD sweep cap    -> LAPACKException retry path      */
+  TTC_ENOTPD = 4,     /* Cholesky breakdown (reserved for the CholeskyQR path)     */
+  TTC_ECUDA = 5,      /* CUDA runtime error                                         */
+  TTC_ENOMEM = 6,     /* device allocation failed                                   */
+  TTC_EINTERNAL = 7,
+  TTC_ENONFINITE = 8  /* NaN or Inf in an input                                     */
+} ttc_status;
+
+enum { TTC_DIR_LEFT = 0, TTC_DIR_RIGHT = 1 };         /* direction=:left / :right      */
+enum { TTC_PREC_FP64 = 0, TTC_PREC_BF16 = 1 };        /* sketch-contraction precision  */
+
+typedef struct ttc_context ttc_context;
+typedef struct ttc_batch ttc_batch;
+
+/* A TTvector in host memory (read-only input). */
+typedef struct {
+  int32_t N;
+  const int64_t* dims;          /* N     */
+  const int64_t* rks;           /* N + 1 */
+  const int64_t* ot;            /* N; may be NULL (= all 0) */
+  const double* const* cores;   /* N host pointers, core k holds dims[k]*rks[k]*rks[k+1] doubles */
+} ttc_ttv;
+
+/* A TTvector result in host memory: the caller allocates core k with room for
+ * dims[k]*rks_cap[k]*rks_cap[k+1] doubles; the library writes the actual core
+ * (dims[k], rks[k], rks[k+1]) packed column-major at the start of the buffer. */
+typedef struct {
+  int32_t N;
+  const int64_t* rks_cap;       /* N + 1, capacities the caller allocated      */
+  int64_t* rks;                 /* N + 1, written                              */
+  int64_t* ot;                  /* N, written                                  */
+  double* const* cores;         /* N host pointers                             */
+} ttc_ttv_out;
+
+/* A TToperator in host memory. */
+typedef struct {
+  int32_t N;
+  const int64_t* dims;          /* N     */
+  const int64_t* rks;           /* N + 1 */
+  const double* const* cores;   /* N host pointers, (n, n, R_{k-1}, R_k) column-major */
+} ttc_tto;
+
+/* Keywords of tt_rounding (src/tt_rounding.jl:146): tol, rmax, direction. */
+typedef struct {
+  double tol;
+  int64_t rmax;
+  int32_t direction;            /* TTC_DIR_LEFT or TTC_DIR_RIGHT */
+} ttc_round_opts;
+
+/* Keywords of ttrand_rounding / tt_recursive_sketch (src/tt_randtools.jl:112,
+ * src/sketches.jl:175): orthogonal, seed, block_rks, plus the arithmetic of the
+ * sketch contractions.  sketch_blocks, when not NULL, supplies the N raw sketch
+ * blocks (b_{k+1}, n_k, b_k, p_k) in Julia layout (already orthogonalised and
+ * scaled as generate_sketch_blocks returns them, src/sketches.jl:44-84), so that
+ * host and device use identical sketches; when NULL the device draws them with
+ * Philox4x32-10 keyed by `seed` (stream = site index). */
+typedef struct {
+  int32_t orthogonal;
+  uint64_t seed;
+  int64_t block_rks;            /* <= 0 means N (the reference default)  */
+  int32_t precision;            /* TTC_PREC_FP64 or TTC_PREC_BF16         */
+  const double* const* sketch_blocks;
+} ttc_sketch_opts;
+
+/* Per-stage device times of the last call (CUDA events on the context stream), ms. */
+typedef struct {
+  double total_ms;
+  double sketch_ms;
+  double orth_ms;     /* QR sweep (deterministic) or orthogonalise-and-project sweep */
+  double svd_ms;      /* truncated-SVD sweep */
+  double h2d_ms;
+  double d2h_ms;
+  int64_t kernel_launches;
+} ttc_stats;
+
+/* ---- context (no reference counterpart: the reference runs in one Julia process) ---- */
+int ttc_create(ttc_context** ctx, int device);
+int ttc_destroy(ttc_context* ctx);
+int ttc_set_stream(ttc_context* ctx, void* cuda_stream);
+const char* ttc_last_error(const ttc_context* ctx);
+int ttc_get_stats(const ttc_context* ctx, ttc_stats* out);
+int ttc_synchronize(ttc_context* ctx);
+/* Library build string, e.g. "libttcuda sm_100a". */
+const char* ttc_version(void);
+
+/* ---- device batches of TTvectors (same N and dims; per-TT capacities) ----
+ * Replaces the Vector{TTvector} the Krylov callers hold (src/tt_solvers.jl:216-218). */
+int ttc_batch_create(ttc_context* ctx, int32_t count, int32_t N, const int64_t* dims,
+                     const int64_t* rks_cap /* count*(N+1) */, ttc_batch** out);
+int ttc_batch_destroy(ttc_batch* b);
+/* TTvector(N, vec, dims, rks, ot) constructor, src/tt_tools.jl:24-34: uploads one TT. */
+int ttc_batch_upload(ttc_batch* b, int32_t index, const ttc_ttv* x);
+int ttc_batch_download(ttc_batch* b, int32_t index, ttc_ttv_out* y);
+/* Upload/download all `count` TTs of the batch in one staged transfer each. */
+int ttc_batch_upload_all(ttc_batch* b, const ttc_ttv* xs);
+int ttc_batch_download_all(ttc_batch* b, ttc_ttv_out* ys);
+int ttc_batch_ranks(ttc_batch* b, int32_t index, int64_t* rks /* N+1 */);
+/* Bytes of device memory held by the batch (cores + rank arrays). */
+size_t ttc_batch_bytes(const ttc_batch* b);
+
+/* tt_rounding(x; tol, rmax, direction) on every TT of a device batch,
+ * src/tt_rounding.jl:146-154 and _tt_rounding :174-269.  `y` must have the same
+ * count/N/dims and capacities >= those of x.  Left-orthogonality of x is taken
+ * from the ot flags uploaded with it (is_leftorthogonal, src/tt_tools.jl:364-367). */
+int ttc_batch_round_det(ttc_context* ctx, ttc_batch* x, const ttc_round_opts* opts, ttc_batch* y);
+/* Same, enqueued on the context stream without the final synchronisation (device-resident
+ * pipelines and timing); errors raised on the device are reported by ttc_synchronize. */
+int ttc_batch_round_det_async(ttc_context* ctx, ttc_batch* x, const ttc_round_opts* opts, ttc_batch* y);
+
+/* ttrand_rounding(y, rks; orthogonal, seed, block_rks) on every TT of a batch,
+ * src/tt_randtools.jl:112-154, followed (when opts_after != NULL) by the
+ * tt_rounding(.; tol) SVD sweep its callers run (src/tt_randtools.jl:476-480).
+ * rks: N+1 target sketch ranks shared by the batch (default_rank_heuristic of the
+ * batch, src/tt_randtools.jl:40-50, is computed by the caller). */
+int ttc_batch_round_rand(ttc_context* ctx, ttc_batch* x, const int64_t* rks,
+                         const ttc_sketch_opts* sk, const ttc_round_opts* opts_after,
+                         ttc_batch* y);
+int ttc_batch_round_rand_async(ttc_context* ctx, ttc_batch* x, const int64_t* rks,
+                               const ttc_sketch_opts* sk, const ttc_round_opts* opts_after,
+                               ttc_batch* y);
+
+/* ---- one-shot entry points on host tensors (a Julia ccall binds these) ---- */
+
+/* tt_rounding(x; tol, rmax, direction), src/tt_rounding.jl:146.  Output ranks are at
+ * most r_and_d_to_rks(x.rks) (src/tt_rounding.jl:6-24); capacity x.rks suffices. */
+int ttc_tt_rounding(ttc_context* ctx, const ttc_ttv* x, const ttc_round_opts* opts, ttc_ttv_out* y);
+
+/* orthogonalize(x; i), src/tt_rounding.jl:65-97 (1-based root i). */
+int ttc_orthogonalize(ttc_context* ctx, const ttc_ttv* x, int32_t i, ttc_ttv_out* y);
+
+/* norm(x), src/tt_rounding.jl:107-114. */
+int ttc_norm(ttc_context* ctx, const ttc_ttv* x, double* out);
+
+/* tt_recursive_sketch(T, A, rks; orthogonal, reverse=true, seed, block_rks),
+ * src/sketches.jl:175-305.  W[k] (k = 0..N) is written column-major
+ * (rks_A[k], sketch_rks[k]) into W_out[k]; sketch_rks (N+1) is returned. */
+int ttc_recursive_sketch(ttc_context* ctx, const ttc_ttv* A, const int64_t* rks,
+                         const ttc_sketch_opts* sk, double* const* W_out, int64_t* sketch_rks);
+
+/* tt_recursive_sketch(T, H, A, rks; ...), src/sketches.jl:317-461: W[k] written as
+ * (rks_A[k], rks_H[k], sketch_rks[k]) column-major. */
+int ttc_recursive_sketch_op(ttc_context* ctx, const ttc_tto* H, const ttc_ttv* A, const int64_t* rks,
+                            const ttc_sketch_opts* sk, double* const* W_out, int64_t* sketch_rks);
+
+/* ttrand_rounding(y, rks; ...), src/tt_randtools.jl:112-154.  Output ranks are
+ * min(n*rho_k, sketch_rks[k+1]) (capacity: the sketch ranks). */
+int ttc_ttrand_rounding(ttc_context* ctx, const ttc_ttv* x, const int64_t* rks,
+                        const ttc_sketch_opts* sk, ttc_ttv_out* y);
+
+/* ttrand_rounding(alpha, ys, rks; ...), src/tt_randtools.jl:223-276. */
+int ttc_ttrand_rounding_lincomb(ttc_context* ctx, int32_t m, const double* alpha, const ttc_ttv* ys,
+                                const int64_t* rks, const ttc_sketch_opts* sk, ttc_ttv_out* y);
+
+/* ttrand_rounding(alpha, A, ys, rks; ...), src/tt_randtools.jl:285-354:
+ * rounding of alpha_1 A ys[0] + sum_{j>0} alpha_j ys[j] without forming A ys[0]. */
+int ttc_ttrand_rounding_op(ttc_context* ctx, int32_t m, const double* alpha, const ttc_tto* A,
+                           const ttc_ttv* ys, const int64_t* rks, const ttc_sketch_opts* sk,
+                           ttc_ttv_out* y);
+
+/* ttrand_rounding(Atto, y, b, rks; ...), src/tt_randtools.jl:169-214: rounding of A y - b. */
+int ttc_ttrand_rounding_residual(ttc_context* ctx, const ttc_tto* A, const ttc_ttv* x, const ttc_ttv* b,
+                                 const int64_t* rks, const ttc_sketch_opts* sk, ttc_ttv_out* y);
+
+/* *(A::TToperator, v::TTvector), src/tt_operations.jl:170-194.  Output ranks
+ * R_k * r_k with the operator index fastest; ot = 0. */
+int ttc_mpo_apply(ttc_context* ctx, const ttc_tto* A, const ttc_ttv* x, ttc_ttv_out* y);
+
+/* dot(A, B), src/tt_operations.jl:302-323. */
+int ttc_dot(ttc_context* ctx, const ttc_ttv* A, const ttc_ttv* B, double* out);
+
+/* partial_contraction(A, B; reverse), src/sketches.jl:1047-1070: W[k] (r^A_k x r^B_k). */
+int ttc_partial_contraction(ttc_context* ctx, const ttc_ttv* A, const ttc_ttv* B, int32_t reverse,
+                            double* const* W_out);
+
+/* dot_operator(psi, H, phi) = <psi|H|phi>, src/tt_operations.jl:390-421. */
+int ttc_dot_operator(ttc_context* ctx, const ttc_ttv* psi, const ttc_tto* H, const ttc_ttv* phi,
+                     double* out);
+
+/* +(x::TTvector, y::TTvector), src/tt_operations.jl:81-112 (direct sum). */
+int ttc_tt_add(ttc_context* ctx, const ttc_ttv* x, const ttc_ttv* y, ttc_ttv_out* out);
+
+/* *(a::Number, A::TTvector), src/tt_operations.jl:428-441 (scales the first ot==0 core). */
+int ttc_tt_scale(ttc_context* ctx, double a, const ttc_ttv* x, ttc_ttv_out* out);
+
+/* Gradient of R(x) = <x|H|x>/<x|x> with respect to every core (H symmetric).
+ * No reference method: it is assembled from the environment contractions of
+ * src/als.jl:9-25 and dot_operator.  grads[k] has the layout of core k.
+ * ckpt_every > 0 stores only every ckpt_every-th left environment and recomputes
+ * the others (memory O(d/ckpt) environments instead of O(d)). */
+int ttc_rayleigh_grad(ttc_context* ctx, const ttc_tto* H, const ttc_ttv* x, int32_t ckpt_every,
+                      double* value, double* const* grads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TTCUDA_H */

@@ -1,0 +1,536 @@
+// extern "C" boundary of libttcuda (declared in include/ttcuda.h).  Converts exceptions to
+// status codes, moves host tensors in the reference's column-major layout to and from the
+// internal device layout (one pinned staging copy per call, permutation on the device).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "api_impl.cuh"
+#include "regions.cuh"
+
+using namespace ttc;
+
+namespace ttc {
+
+static thread_local std::string g_err_noctx;
+
+template <class F>
+int guard(ttc_context* c, F&& f) {
+  try {
+    if (c) TTC_CUDA(cudaSetDevice(c->device));
+    f();
+    return TTC_OK;
+  } catch (const Error& e) {
+    if (c) c->err = e.what(); else g_err_noctx = e.what();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    if (c) c->err = "host allocation failed"; else g_err_noctx = "host allocation failed";
+    return TTC_ENOMEM;
+  } catch (const std::exception& e) {
+    if (c) c->err = e.what(); else g_err_noctx = e.what();
+    return TTC_EINTERNAL;
+  }
+}
+
+void ensure_stage(ttc_context* c, size_t bytes) {
+  if (bytes <= c->stage_bytes) return;
+  TTC_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->d_stage) { region_remove(c->d_stage); cudaFree(c->d_stage); }
+  if (c->h_stage) cudaFreeHost(c->h_stage);
+  c->d_stage = nullptr; c->h_stage = nullptr; c->stage_bytes = 0;
+  const size_t nb = bytes + bytes / 4 + (1 << 16);
+  if (cudaMalloc(&c->d_stage, nb) != cudaSuccess) { cudaGetLastError(); throw Error(TTC_ENOMEM, "staging allocation failed"); }
+  if (cudaMallocHost(&c->h_stage, nb) != cudaSuccess) { cudaGetLastError(); throw Error(TTC_ENOMEM, "pinned staging allocation failed"); }
+  c->stage_bytes = nb;
+  region_add(c->d_stage, nb);
+}
+
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+void validate_ttv(const ttc_ttv* x) {
+  TTC_REQUIRE(x && x->N > 0 && x->dims && x->rks && x->cores, TTC_EARG, "TTvector: null field");
+  for (int k = 0; k < x->N; ++k) {
+    TTC_REQUIRE(x->dims[k] > 0, TTC_EARG, "TTvector: dims must be positive");
+    TTC_REQUIRE(x->cores[k] != nullptr, TTC_EARG, "TTvector: null core");
+  }
+  TTC_REQUIRE(x->rks[0] == 1 && x->rks[x->N] == 1, TTC_EDIM, "TTvector: boundary ranks must be 1");
+  for (int k = 0; k <= x->N; ++k) TTC_REQUIRE(x->rks[k] >= 1, TTC_EDIM, "TTvector: ranks must be >= 1");
+}
+
+// Upload many TTs into consecutive slots [first, first+m) of a batch.
+void batch_upload_many(ttc_batch* b, int first, int m, const ttc_ttv* xs, bool reverse) {
+  ttc_context* c = b->ctx;
+  const int N = b->N;
+  size_t data = 0;
+  for (int i = 0; i < m; ++i) {
+    const ttc_ttv& x = xs[i];
+    validate_ttv(&x);
+    TTC_REQUIRE(x.N == N, TTC_EDIM, "upload: N differs from the batch");
+    for (int k = 0; k < N; ++k)
+      TTC_REQUIRE(x.dims[reverse ? N - 1 - k : k] == b->dims[k], TTC_EDIM, "upload: dims differ from the batch");
+    for (int k = 0; k <= N; ++k)
+      TTC_REQUIRE(x.rks[reverse ? N - k : k] <= b->capr(first + i, k), TTC_EDIM, "upload: rank exceeds the batch capacity");
+    for (int k = 0; k < N; ++k) data += (size_t)x.dims[k] * x.rks[k] * x.rks[k + 1];
+  }
+  const size_t nd = (size_t)m * N;
+  const size_t off_desc = align_up(data * sizeof(double), 256);
+  const size_t off_rk = align_up(off_desc + nd * sizeof(CopyDesc), 256);
+  const size_t total = off_rk + (size_t)m * (N + 1) * sizeof(int);
+  ensure_stage(c, total);
+  unsigned char* h = (unsigned char*)c->h_stage;
+  unsigned char* d = (unsigned char*)c->d_stage;
+  double* hd = (double*)h;
+  CopyDesc* hc = (CopyDesc*)(h + off_desc);
+  int* hr = (int*)(h + off_rk);
+  size_t o = 0, ci = 0;
+  long long maxe = 0;
+  for (int i = 0; i < m; ++i) {
+    const ttc_ttv& x = xs[i];
+    const int t = first + i;
+    for (int k = 0; k < N; ++k) {
+      const int kx = reverse ? N - 1 - k : k;     // host core feeding slot core k
+      const long long n = x.dims[kx], r0 = x.rks[kx], r1 = x.rks[kx + 1], cap0 = b->capr(t, k);
+      const size_t cnt = (size_t)n * r0 * r1;
+      std::memcpy(hd + o, x.cores[kx], cnt * sizeof(double));
+      // Julia (i, a, b) at i + n*(a + r0*b)  ->  internal (a, i, b) at a + cap0*(i + n*b);
+      // reversed: internal (b, i, a) at b + cap0*(i + n*a)
+      if (!reverse)
+        hc[ci++] = cd3((const double*)(d) + o, b->core(t, k), n, r0, r1, 1, n, n * r0, cap0, 1, cap0 * n);
+      else
+        hc[ci++] = cd3((const double*)(d) + o, b->core(t, k), n, r0, r1, 1, n, n * r0, cap0, cap0 * n, 1);
+      maxe = std::max<long long>(maxe, (long long)cnt);
+      o += cnt;
+    }
+    for (int k = 0; k <= N; ++k) hr[(size_t)i * (N + 1) + k] = (int)x.rks[reverse ? N - k : k];
+  }
+  // zero the slots (padding must be 0), then copy data + descriptors + ranks in one transfer
+  TTC_CUDA(cudaMemsetAsync(b->core(first, 0), 0, sizeof(double) * (b->tt_off[first + m] - b->tt_off[first]), c->stream));
+  TTC_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, c->stream));
+  launch_copy((const CopyDesc*)(d + off_desc), (int)ci, maxe, c->stream);
+  TTC_CUDA(cudaMemcpyAsync(b->drk(first, 0), d + off_rk, (size_t)m * (N + 1) * sizeof(int), cudaMemcpyDeviceToDevice,
+                           c->stream));
+  TTC_CUDA(cudaMemsetAsync(b->d_zero + first, 0, sizeof(int) * m, c->stream));
+  TTC_CUDA(cudaStreamSynchronize(c->stream));   // the pinned staging is reused by the next call
+  unsigned long long hsh = 1469598103934665603ull;
+  for (int i = 0; i < m; ++i) {
+    const ttc_ttv& x = xs[i];
+    const int t = first + i;
+    for (int k = 0; k <= N; ++k) b->h_rks[(size_t)t * (N + 1) + k] = (int)x.rks[reverse ? N - k : k];
+    for (int k = 0; k < N; ++k)
+      b->h_ot[(size_t)t * N + k] = x.ot ? (reverse ? -(int)x.ot[N - 1 - k] : (int)x.ot[k]) : 0;
+  }
+  for (int v : b->h_rks) hsh = (hsh ^ (unsigned)v) * 1099511628211ull;
+  for (int v : b->h_ot) hsh = (hsh ^ (unsigned)(v + 7)) * 1099511628211ull;
+  b->version = hsh;
+  b->rks_dirty = false;
+}
+
+void batch_download_many(ttc_batch* b, int first, int m, ttc_ttv_out* ys, bool reverse) {
+  ttc_context* c = b->ctx;
+  const int N = b->N;
+  batch_sync_ranks(b);
+  size_t data = 0;
+  for (int i = 0; i < m; ++i) {
+    const int t = first + i;
+    TTC_REQUIRE(ys[i].N == N && ys[i].rks && ys[i].cores, TTC_EARG, "download: bad output descriptor");
+    for (int k = 0; k <= N; ++k)
+      if (ys[i].rks_cap)
+        TTC_REQUIRE(b->rk(t, reverse ? N - k : k) <= ys[i].rks_cap[k], TTC_EDIM,
+                    "download: output capacity smaller than the result rank");
+    for (int k = 0; k < N; ++k) data += (size_t)b->dims[k] * b->rk(t, k) * b->rk(t, k + 1);
+  }
+  const size_t nd = (size_t)m * N;
+  const size_t off_desc = align_up(data * sizeof(double), 256);
+  const size_t total = off_desc + nd * sizeof(CopyDesc);
+  ensure_stage(c, total);
+  unsigned char* h = (unsigned char*)c->h_stage;
+  unsigned char* d = (unsigned char*)c->d_stage;
+  CopyDesc* hc = (CopyDesc*)(h + off_desc);
+  size_t o = 0, ci = 0;
+  long long maxe = 0;
+  std::vector<size_t> offs;
+  for (int i = 0; i < m; ++i) {
+    const int t = first + i;
+    for (int ko = 0; ko < N; ++ko) {           // output core ko
+      const int k = reverse ? N - 1 - ko : ko;  // batch core holding it
+      const long long n = b->dims[k], r0 = b->rk(t, k), r1 = b->rk(t, k + 1), cap0 = b->capr(t, k);
+      if (!reverse)
+        hc[ci++] = cd3(b->core(t, k), (double*)d + o, n, r0, r1, cap0, 1, cap0 * n, 1, n, n * r0);
+      else  // output (i, a, b) with a < r1, b < r0 from internal (b, i, a)
+        hc[ci++] = cd3(b->core(t, k), (double*)d + o, n, r1, r0, cap0, cap0 * n, 1, 1, n, n * r1);
+      maxe = std::max<long long>(maxe, n * r0 * r1);
+      offs.push_back(o);
+      o += (size_t)n * r0 * r1;
+    }
+  }
+  TTC_CUDA(cudaMemcpyAsync(d + off_desc, h + off_desc, nd * sizeof(CopyDesc), cudaMemcpyHostToDevice, c->stream));
+  launch_copy((const CopyDesc*)(d + off_desc), (int)ci, maxe, c->stream);
+  TTC_CUDA(cudaMemcpyAsync(h, d, data * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  TTC_CUDA(cudaStreamSynchronize(c->stream));
+  size_t q = 0;
+  for (int i = 0; i < m; ++i) {
+    const int t = first + i;
+    for (int ko = 0; ko < N; ++ko) {
+      const int k = reverse ? N - 1 - ko : ko;
+      const size_t cnt = (size_t)b->dims[k] * b->rk(t, k) * b->rk(t, k + 1);
+      std::memcpy(ys[i].cores[ko], (double*)h + offs[q++], cnt * sizeof(double));
+    }
+    for (int k = 0; k <= N; ++k) ys[i].rks[k] = b->rk(t, reverse ? N - k : k);
+    if (ys[i].ot)
+      for (int k = 0; k < N; ++k)
+        ys[i].ot[k] = reverse ? -b->h_ot[(size_t)t * N + (N - 1 - k)] : b->h_ot[(size_t)t * N + k];
+  }
+}
+
+// A one-TT batch holding the host tensor x, with capacities max(cap, x.rks).
+ttc_batch* batch_from_host(ttc_context* c, const ttc_ttv* x, const std::vector<int>* cap, bool reverse) {
+  validate_ttv(x);
+  const int N = x->N;
+  std::vector<long long> dims(N);
+  for (int k = 0; k < N; ++k) dims[k] = x->dims[reverse ? N - 1 - k : k];
+  std::vector<int> cp(N + 1);
+  for (int k = 0; k <= N; ++k) cp[k] = std::max<int>((int)x->rks[reverse ? N - k : k], cap ? (*cap)[k] : 1);
+  ttc_batch* b = batch_create(c, 1, N, dims.data(), cp.data());
+  try {
+    batch_upload_many(b, 0, 1, x, reverse);
+  } catch (...) {
+    batch_destroy(b);
+    throw;
+  }
+  return b;
+}
+
+ttc_batch* batch_empty_like(ttc_context* c, int count, int N, const std::vector<long long>& dims,
+                            const std::vector<int>& cap_per_tt) {
+  std::vector<int> cp;
+  for (int t = 0; t < count; ++t) cp.insert(cp.end(), cap_per_tt.begin(), cap_per_tt.end());
+  return batch_create(c, count, N, dims.data(), cp.data());
+}
+
+
+
+void record_stats(ttc_context* c, int nstages) {
+  TTC_CUDA(cudaStreamSynchronize(c->stream));
+  float ms[8] = {0};
+  for (int i = 0; i + 1 < nstages; ++i) cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]);
+  float tot = 0;
+  cudaEventElapsedTime(&tot, c->ev[0], c->ev[nstages - 1]);
+  c->stats.total_ms = tot;
+  c->stats.sketch_ms = 0; c->stats.orth_ms = 0; c->stats.svd_ms = 0;
+  if (nstages == 3) { c->stats.orth_ms = ms[0]; c->stats.svd_ms = ms[1]; }
+  if (nstages == 4) { c->stats.sketch_ms = ms[0]; c->stats.orth_ms = ms[1]; c->stats.svd_ms = ms[2]; }
+}
+
+std::vector<const double*> upload_host_blocks(ttc_context* c, const std::vector<long long>& dims, const SketchPlan& sp,
+                                              const double* const* blocks, std::string& key) {
+  std::vector<const double*> out;
+  if (!blocks) return out;
+  const int N = (int)dims.size();
+  size_t total = 0;
+  for (int k = 0; k < N; ++k) total += (size_t)sp.b[k + 1] * dims[k] * sp.b[k] * sp.p[k];
+  if (total > c->sk_cap) {
+    if (c->d_sk) { region_remove(c->d_sk); cudaFree(c->d_sk); }
+    c->d_sk = nullptr;
+    TTC_CUDA(cudaMalloc(&c->d_sk, total * sizeof(double)));
+    region_add(c->d_sk, total * sizeof(double));
+    c->sk_cap = total;
+  }
+  size_t o = 0;
+  for (int k = 0; k < N; ++k) {
+    TTC_REQUIRE(blocks[k] != nullptr, TTC_EARG, "sketch_blocks: null block");
+    const size_t cnt = (size_t)sp.b[k + 1] * dims[k] * sp.b[k] * sp.p[k];
+    TTC_CUDA(cudaMemcpyAsync(c->d_sk + o, blocks[k], cnt * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    out.push_back(c->d_sk + o);
+    o += cnt;
+  }
+  TTC_CUDA(cudaStreamSynchronize(c->stream));
+  key = "hostsk:" + std::to_string((unsigned long long)(uintptr_t)c->d_sk) + ":";
+  return out;
+}
+
+std::vector<long long> rks_vec(const int64_t* rks, int N) {
+  TTC_REQUIRE(rks != nullptr, TTC_EARG, "rks is null");
+  return std::vector<long long>(rks, rks + N + 1);
+}
+
+}  // namespace ttc
+
+// ================================================================= extern "C"
+extern "C" {
+
+const char* ttc_version(void) { return "libttcuda 0.1 sm_100a (tcgen05 BF16 sketch, FP64 QR/Jacobi)"; }
+
+int ttc_create(ttc_context** out, int device) {
+  if (!out) return TTC_EARG;
+  ttc_context* c = new (std::nothrow) ttc_context();
+  if (!c) return TTC_ENOMEM;
+  c->device = device;
+  const int st = guard(c, [&] {
+    int n = 0;
+    TTC_CUDA(cudaGetDeviceCount(&n));
+    TTC_REQUIRE(device >= 0 && device < n, TTC_EARG, "ttc_create: no such device");
+    TTC_CUDA(cudaSetDevice(device));
+    TTC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
+    TTC_CUDA(cudaMalloc(&c->d_flags, 64));
+    region_add(c->d_flags, 64);
+    TTC_CUDA(cudaMemset(c->d_flags, 0, 64));
+    TTC_CUDA(cudaMalloc(&c->d_one, 64));
+    region_add(c->d_one, 64);
+    const double one[8] = {1.0, 0, 0, 0, 0, 0, 0, 0};
+    TTC_CUDA(cudaMemcpy(c->d_one, one, sizeof(one), cudaMemcpyHostToDevice));
+    for (auto& e : c->ev) TTC_CUDA(cudaEventCreate(&e));
+  });
+  if (st != TTC_OK) {
+    g_err_noctx = c->err;
+    delete c;
+    return st;
+  }
+  *out = c;
+  return TTC_OK;
+}
+
+int ttc_destroy(ttc_context* c) {
+  if (!c) return TTC_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->plans.clear();
+  for (void* p : {(void*)c->ws, c->d_stage, (void*)c->d_sk, (void*)c->d_flags, (void*)c->d_one}) region_remove(p);
+  if (c->ws) cudaFree(c->ws);
+  if (c->d_stage) cudaFree(c->d_stage);
+  if (c->h_stage) cudaFreeHost(c->h_stage);
+  if (c->d_sk) cudaFree(c->d_sk);
+  if (c->d_flags) cudaFree(c->d_flags);
+  if (c->d_one) cudaFree(c->d_one);
+  for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return TTC_OK;
+}
+
+int ttc_set_stream(ttc_context* c, void* stream) {
+  if (!c) return TTC_EARG;
+  return guard(c, [&] {
+    TTC_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+  });
+}
+
+const char* ttc_last_error(const ttc_context* c) { return c ? c->err.c_str() : g_err_noctx.c_str(); }
+
+int ttc_get_stats(const ttc_context* c, ttc_stats* out) {
+  if (!c || !out) return TTC_EARG;
+  *out = c->stats;
+  return TTC_OK;
+}
+
+int ttc_synchronize(ttc_context* c) {
+  if (!c) return TTC_EARG;
+  return guard(c, [&] {
+    TTC_CUDA(cudaStreamSynchronize(c->stream));
+    check_device_flags(c);
+  });
+}
+
+int ttc_batch_create(ttc_context* c, int32_t count, int32_t N, const int64_t* dims, const int64_t* rks_cap,
+                     ttc_batch** out) {
+  if (!c || !out || !dims || !rks_cap) return TTC_EARG;
+  return guard(c, [&] {
+    std::vector<long long> d(dims, dims + N);
+    std::vector<int> cp((size_t)count * (N + 1));
+    for (size_t i = 0; i < cp.size(); ++i) {
+      TTC_REQUIRE(rks_cap[i] >= 1 && rks_cap[i] < (1 << 20), TTC_EARG, "batch: bad capacity");
+      cp[i] = (int)rks_cap[i];
+    }
+    for (int t = 0; t < count; ++t)
+      TTC_REQUIRE(cp[(size_t)t * (N + 1)] == 1 && cp[(size_t)t * (N + 1) + N] == 1, TTC_EDIM,
+                  "batch: boundary capacities must be 1");
+    *out = batch_create(c, count, N, d.data(), cp.data());
+  });
+}
+
+int ttc_batch_destroy(ttc_batch* b) {
+  if (!b) return TTC_OK;
+  ttc_context* c = b->ctx;
+  return guard(c, [&] {
+    TTC_CUDA(cudaStreamSynchronize(c->stream));
+    batch_destroy(b);
+  });
+}
+
+int ttc_batch_upload(ttc_batch* b, int32_t index, const ttc_ttv* x) {
+  if (!b || !x) return TTC_EARG;
+  return guard(b->ctx, [&] {
+    TTC_REQUIRE(index >= 0 && index < b->count, TTC_EARG, "upload: index out of range");
+    batch_upload_many(b, index, 1, x);
+  });
+}
+
+int ttc_batch_upload_all(ttc_batch* b, const ttc_ttv* xs) {
+  if (!b || !xs) return TTC_EARG;
+  return guard(b->ctx, [&] { batch_upload_many(b, 0, b->count, xs); });
+}
+
+int ttc_batch_download(ttc_batch* b, int32_t index, ttc_ttv_out* y) {
+  if (!b || !y) return TTC_EARG;
+  return guard(b->ctx, [&] {
+    TTC_REQUIRE(index >= 0 && index < b->count, TTC_EARG, "download: index out of range");
+    check_device_flags(b->ctx);
+    batch_download_many(b, index, 1, y);
+  });
+}
+
+int ttc_batch_download_all(ttc_batch* b, ttc_ttv_out* ys) {
+  if (!b || !ys) return TTC_EARG;
+  return guard(b->ctx, [&] {
+    check_device_flags(b->ctx);
+    batch_download_many(b, 0, b->count, ys);
+  });
+}
+
+int ttc_batch_ranks(ttc_batch* b, int32_t index, int64_t* rks) {
+  if (!b || !rks) return TTC_EARG;
+  return guard(b->ctx, [&] {
+    TTC_REQUIRE(index >= 0 && index < b->count, TTC_EARG, "ranks: index out of range");
+    batch_sync_ranks(b);
+    for (int k = 0; k <= b->N; ++k) rks[k] = b->rk(index, k);
+  });
+}
+
+size_t ttc_batch_bytes(const ttc_batch* b) {
+  if (!b) return 0;
+  return sizeof(double) * (size_t)b->total + sizeof(int) * (b->h_rks.size() + b->count);
+}
+
+int ttc_batch_round_det(ttc_context* c, ttc_batch* x, const ttc_round_opts* opts, ttc_batch* y) {
+  if (!c || !x || !y || !opts) return TTC_EARG;
+  return guard(c, [&] {
+    round_det(c, x, *opts, y);
+    record_stats(c, 3);
+    check_device_flags(c);
+  });
+}
+
+int ttc_batch_round_det_async(ttc_context* c, ttc_batch* x, const ttc_round_opts* opts, ttc_batch* y) {
+  if (!c || !x || !y || !opts) return TTC_EARG;
+  return guard(c, [&] { round_det(c, x, *opts, y); });
+}
+
+int ttc_batch_round_rand(ttc_context* c, ttc_batch* x, const int64_t* rks, const ttc_sketch_opts* sk,
+                         const ttc_round_opts* after, ttc_batch* y) {
+  if (!c || !x || !y || !sk) return TTC_EARG;
+  return guard(c, [&] {
+    std::string key;
+    const auto r = rks_vec(rks, x->N);
+    const auto raw = upload_host_blocks(c, x->dims, sketch_plan(x->dims, r, sk->block_rks), sk->sketch_blocks, key);
+    round_rand(c, x, r, *sk, after, y, raw, key);
+    record_stats(c, 4);
+    check_device_flags(c);
+  });
+}
+
+int ttc_batch_round_rand_async(ttc_context* c, ttc_batch* x, const int64_t* rks, const ttc_sketch_opts* sk,
+                               const ttc_round_opts* after, ttc_batch* y) {
+  if (!c || !x || !y || !sk) return TTC_EARG;
+  return guard(c, [&] {
+    TTC_REQUIRE(sk->sketch_blocks == nullptr, TTC_EARG, "async rounding takes device-generated sketches only");
+    round_rand(c, x, rks_vec(rks, x->N), *sk, after, y, {}, "");
+  });
+}
+
+int ttc_tt_rounding(ttc_context* c, const ttc_ttv* x, const ttc_round_opts* opts, ttc_ttv_out* y) {
+  if (!c || !x || !opts || !y) return TTC_EARG;
+  return guard(c, [&] { tt_rounding_host(c, x, *opts, y); });
+}
+
+int ttc_orthogonalize(ttc_context* c, const ttc_ttv* x, int32_t i, ttc_ttv_out* y) {
+  if (!c || !x || !y) return TTC_EARG;
+  return guard(c, [&] { orthogonalize_host(c, x, i, y); });
+}
+
+int ttc_norm(ttc_context* c, const ttc_ttv* x, double* out) {
+  if (!c || !x || !out) return TTC_EARG;
+  return guard(c, [&] { *out = norm_host(c, x); });
+}
+
+int ttc_recursive_sketch(ttc_context* c, const ttc_ttv* A, const int64_t* rks, const ttc_sketch_opts* sk,
+                         double* const* W_out, int64_t* sketch_rks) {
+  if (!c || !A || !sk || !W_out || !sketch_rks) return TTC_EARG;
+  return guard(c, [&] { recursive_sketch_host(c, A, nullptr, rks, *sk, W_out, sketch_rks); });
+}
+
+int ttc_recursive_sketch_op(ttc_context* c, const ttc_tto* H, const ttc_ttv* A, const int64_t* rks,
+                            const ttc_sketch_opts* sk, double* const* W_out, int64_t* sketch_rks) {
+  if (!c || !H || !A || !sk || !W_out || !sketch_rks) return TTC_EARG;
+  return guard(c, [&] { recursive_sketch_host(c, A, H, rks, *sk, W_out, sketch_rks); });
+}
+
+int ttc_ttrand_rounding(ttc_context* c, const ttc_ttv* x, const int64_t* rks, const ttc_sketch_opts* sk, ttc_ttv_out* y) {
+  if (!c || !x || !sk || !y) return TTC_EARG;
+  return guard(c, [&] {
+    const double one = 1.0;
+    rand_rounding_host(c, 1, &one, nullptr, x, nullptr, rks, *sk, y);
+  });
+}
+
+int ttc_ttrand_rounding_lincomb(ttc_context* c, int32_t m, const double* alpha, const ttc_ttv* ys, const int64_t* rks,
+                                const ttc_sketch_opts* sk, ttc_ttv_out* y) {
+  if (!c || m < 1 || !alpha || !ys || !sk || !y) return TTC_EARG;
+  return guard(c, [&] { rand_rounding_host(c, m, alpha, nullptr, ys, nullptr, rks, *sk, y); });
+}
+
+int ttc_ttrand_rounding_op(ttc_context* c, int32_t m, const double* alpha, const ttc_tto* A, const ttc_ttv* ys,
+                           const int64_t* rks, const ttc_sketch_opts* sk, ttc_ttv_out* y) {
+  if (!c || m < 1 || !alpha || !A || !ys || !sk || !y) return TTC_EARG;
+  return guard(c, [&] { rand_rounding_host(c, m, alpha, A, ys, nullptr, rks, *sk, y); });
+}
+
+int ttc_ttrand_rounding_residual(ttc_context* c, const ttc_tto* A, const ttc_ttv* x, const ttc_ttv* b,
+                                 const int64_t* rks, const ttc_sketch_opts* sk, ttc_ttv_out* y) {
+  if (!c || !A || !x || !b || !sk || !y) return TTC_EARG;
+  return guard(c, [&] {
+    const double al[2] = {1.0, -1.0};
+    const ttc_ttv ys[2] = {*x, *b};
+    rand_rounding_host(c, 2, al, A, ys, nullptr, rks, *sk, y);
+  });
+}
+
+int ttc_mpo_apply(ttc_context* c, const ttc_tto* A, const ttc_ttv* x, ttc_ttv_out* y) {
+  if (!c || !A || !x || !y) return TTC_EARG;
+  return guard(c, [&] { mpo_apply_host(c, A, x, y); });
+}
+
+int ttc_dot(ttc_context* c, const ttc_ttv* A, const ttc_ttv* B, double* out) {
+  if (!c || !A || !B || !out) return TTC_EARG;
+  return guard(c, [&] { *out = dot_host(c, A, B, nullptr, 1); });
+}
+
+int ttc_partial_contraction(ttc_context* c, const ttc_ttv* A, const ttc_ttv* B, int32_t reverse, double* const* W_out) {
+  if (!c || !A || !B || !W_out) return TTC_EARG;
+  return guard(c, [&] { dot_host(c, A, B, W_out, reverse); });
+}
+
+int ttc_dot_operator(ttc_context* c, const ttc_ttv* psi, const ttc_tto* H, const ttc_ttv* phi, double* out) {
+  if (!c || !psi || !H || !phi || !out) return TTC_EARG;
+  return guard(c, [&] { *out = dot_operator_host(c, psi, H, phi); });
+}
+
+int ttc_tt_add(ttc_context* c, const ttc_ttv* x, const ttc_ttv* y, ttc_ttv_out* out) {
+  if (!c || !x || !y || !out) return TTC_EARG;
+  return guard(c, [&] { tt_add_host(c, x, y, out); });
+}
+
+int ttc_tt_scale(ttc_context* c, double a, const ttc_ttv* x, ttc_ttv_out* out) {
+  if (!c || !x || !out) return TTC_EARG;
+  return guard(c, [&] { tt_scale_host(c, a, x, out); });
+}
+
+int ttc_rayleigh_grad(ttc_context* c, const ttc_tto* H, const ttc_ttv* x, int32_t ckpt_every, double* value,
+                      double* const* grads) {
+  if (!c || !H || !x || !value || !grads) return TTC_EARG;
+  return guard(c, [&] { rayleigh_grad_host(c, H, x, ckpt_every, value, grads); });
+}
+
+}  // extern "C"

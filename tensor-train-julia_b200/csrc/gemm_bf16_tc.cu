@@ -1,0 +1,245 @@
+// Grouped BF16 GEMM on the 5th-generation tensor cores (tcgen05, sm_100a), FP32
+// accumulation in tensor memory.  Used for the reverse-sketch contractions of
+// tt_recursive_sketch (src/sketches.jl:1602-1638) in the mixed-precision rounding:
+//   C(i, j) = alpha * sum_k A(i, k) * B(j, k),   A and B K-major BF16 (row stride lda/ldb,
+//   a multiple of 8 elements, K zero padded to a multiple of 8).
+// Tile 128 x 128 x 64, one CTA (4 warps) per output tile.  Operand tiles are staged with
+// cp.async into the 128-byte-swizzled K-major layout that the UMMA shared-memory
+// descriptors describe; one elected thread issues tcgen05.mma (M=128, N=128, K=16) and
+// tcgen05.commit arrives on an mbarrier; a two-stage ring overlaps the next tile's loads
+// with the current MMAs.  The epilogue reads the accumulator with tcgen05.ld (32x32b)
+// and writes FP64 / FP32 / BF16 outputs with arbitrary (split) strides.
+// Every mbarrier wait is bounded: on timeout the kernel raises DFLAG_TIMEOUT, frees its
+// tensor memory and returns.
+#include <cuda_bf16.h>
+
+#include "kernels.cuh"
+
+namespace ttc {
+namespace {
+constexpr int BM = 128, BN = 128, BK = 64, NT = 128, STAGES = 2;
+constexpr int TILE_BYTES = BM * BK * 2;                 // 16 KB per operand tile
+constexpr uint32_t TMEM_COLS = 128;
+constexpr long long WAIT_LIMIT = 1LL << 24;             // bounded mbarrier polls
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void cp_async_16(uint32_t dst, const void* src, bool valid) {
+  const int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait; returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < WAIT_LIMIT; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t make_sdesc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);            // start address
+  d |= (uint64_t)1 << 16;                             // leading byte offset (unused for SW128 K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;                   // stride byte offset
+  d |= (uint64_t)1 << 46;                             // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                             // layout: SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor, kind::f16: D=F32, A=B=BF16, both K-major, M=128, N=128.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ int find_desc(const Bf16GemmDesc* __restrict__ d, int nd, long long tile) {
+  int lo = 0, hi = nd - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (d[mid].tile_start <= tile) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+}  // namespace
+
+__global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc* __restrict__ descs, int nd, int* flags) {
+  extern __shared__ __align__(1024) unsigned char dsm[];
+  __shared__ uint64_t mbar[STAGES];
+  __shared__ uint32_t tmem_base_sh;
+  // 1024-byte aligned operand ring
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(dsm) + 1023) & ~uintptr_t(1023));
+  unsigned char* As = base;
+  unsigned char* Bs = base + STAGES * TILE_BYTES;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long tile = blockIdx.x;
+  const Bf16GemmDesc D = descs[find_desc(descs, nd, tile)];
+  const int tm = (D.m + BM - 1) / BM, tn = (D.n + BN - 1) / BN;
+  const long long local = tile - D.tile_start;
+  if (local < 0 || local >= (long long)tm * tn) return;
+  const int bm = (int)(local % tm), bn = (int)(local / tm);
+  const int row0 = bm * BM, col0 = bn * BN;
+  const int nk = (D.k + BK - 1) / BK;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(smem_u32(&mbar[s]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+
+  const __nv_bfloat16* Ag = reinterpret_cast<const __nv_bfloat16*>(D.A);
+  const __nv_bfloat16* Bg = reinterpret_cast<const __nv_bfloat16*>(D.B);
+
+  // Each thread moves 8 of the 1024 16-byte chunks of each operand tile.
+  auto load_stage = [&](int kt, int s) {
+    const int k0 = kt * BK;
+    const uint32_t sa = smem_u32(As + s * TILE_BYTES), sb = smem_u32(Bs + s * TILE_BYTES);
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const int idx = tid + NT * t;          // 0..1023
+      const int r = idx >> 3, c = idx & 7;   // row, 16-byte chunk within the 128-byte row
+      const int kk = k0 + c * 8;
+      const uint32_t off = (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
+      const int gi = row0 + r, gj = col0 + r;
+      const bool va = (gi < D.m) && (kk < D.k);
+      const bool vb = (gj < D.n) && (kk < D.k);
+      cp_async_16(sa + off, va ? (const void*)(Ag + (long long)gi * D.lda + kk) : (const void*)Ag, va);
+      cp_async_16(sb + off, vb ? (const void*)(Bg + (long long)gj * D.ldb + kk) : (const void*)Bg, vb);
+    }
+    cp_async_commit();
+  };
+
+  bool ok = true;
+  load_stage(0, 0);
+  for (int kt = 0; kt < nk; ++kt) {
+    const int s = kt & 1;
+    if (kt + 1 < nk) {
+      // stage s^1 was read by the MMAs of iteration kt-1
+      if (kt >= 1) ok = ok && mbar_wait(smem_u32(&mbar[s ^ 1]), (uint32_t)(((kt - 1) >> 1) & 1));
+      load_stage(kt + 1, s ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0 && ok) {
+      tc_fence_after();
+      const uint32_t sa = smem_u32(As + s * TILE_BYTES), sb = smem_u32(Bs + s * TILE_BYTES);
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk) {
+        umma_bf16(tmem, make_sdesc(sa + kk * 32), make_sdesc(sb + kk * 32), (kt > 0 || kk > 0) ? 1u : 0u);
+      }
+      umma_commit(smem_u32(&mbar[s]));
+    }
+    __syncthreads();
+  }
+  if (nk > 0) ok = ok && mbar_wait(smem_u32(&mbar[(nk - 1) & 1]), (uint32_t)(((nk - 1) >> 1) & 1));
+  ok = __syncthreads_and(ok) != 0;
+  if (!ok && nk > 0) mbar_wait(smem_u32(&mbar[(nk - 1) & 1]), (uint32_t)(((nk - 1) >> 1) & 1));  // drain, bounded
+  tc_fence_after();
+  if (!ok) {
+    if (tid == 0) atomicOr(flags, DFLAG_TIMEOUT);
+  } else {
+    // Epilogue: warp w owns accumulator rows 32w..32w+31 (TMEM lanes).
+    const int row = row0 + warp * 32 + lane;
+    const long long roff64 = (long long)(row % D.m0) * D.c_i0 + (long long)(row / D.m0) * D.c_i1;
+    const long long roff16 = (long long)(row % D.m0) * D.h_i0 + (long long)(row / D.m0) * D.h_i1;
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      float v[16];
+      if (nk > 0) tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = 0.f;
+      }
+      if (row < D.m) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int col = col0 + c0 + i;
+          if (col < D.n) {
+            const double x = D.alpha * (double)v[i];
+            if (D.C64) D.C64[roff64 + (long long)col * D.c_j] = x;
+            if (D.C32) reinterpret_cast<float*>(D.C32)[roff64 + (long long)col * D.c_j] = (float)x;
+            if (D.C16) reinterpret_cast<__nv_bfloat16*>(D.C16)[roff16 + (long long)col * D.h_j] = __double2bfloat16(x);
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+long long bf16_gemm_tiles(const Bf16GemmDesc& d) {
+  if (d.m <= 0 || d.n <= 0) return 0;
+  return (long long)((d.m + BM - 1) / BM) * ((d.n + BN - 1) / BN);
+}
+
+void launch_gemm_bf16_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags) {
+  if (nd <= 0 || total_tiles <= 0) return;
+  const int smem = STAGES * 2 * TILE_BYTES + 1024;
+  static bool attr = false;
+  if (!attr) {
+    TTC_CUDA(cudaFuncSetAttribute(gemm_bf16_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  gemm_bf16_tc_kernel<<<(unsigned)total_tiles, NT, smem, s>>>(d, nd, d_flags);
+  TTC_CHECK_LAUNCH();
+}
+
+}  // namespace ttc

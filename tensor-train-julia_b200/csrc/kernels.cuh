@@ -1,0 +1,108 @@
+// Launchers of the device kernels of libttcuda (all FP64 unless stated).
+#pragma once
+#include "common.cuh"
+
+namespace ttc {
+
+// ---- grouped FP64 GEMM (gemm_f64.cu)
+void launch_gemm_f64(const GemmDesc* d_descs, int nd, long long total_tiles, cudaStream_t s);
+long long gemm_tiles(const GemmDesc& d);
+
+// ---- batched Householder QR (qr_householder.cu)
+// A (m x n, col-major, lda) is overwritten.  Q (m x K, ldq) and R (K x n, ldr),
+// K = min(m, n), like LAPACK geqrf + orgqr (Julia `qr`, `Matrix(F.Q)`, `F.R`).
+// Q == nullptr skips the Q formation, R == nullptr skips R.
+struct QRDesc {
+  int m, n;
+  double* A; int lda;
+  double* Q; int ldq;
+  double* R; int ldr;
+  double* Tws;      // >= ceil(K/16)*16*16 doubles of workspace for the block reflectors
+};
+constexpr int QR_MAX_M = 1536;
+void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags);
+
+// ---- batched one-sided Jacobi SVD (svd_jacobi.cu)
+// X (m x n, col-major, ldx, m >= n) is overwritten by X*W whose columns are
+// orthogonal; W (n x n, ldw) accumulates the rotations when not null.
+// sigma[i] = ||column i||; perm lists columns by decreasing sigma.
+struct JacobiDesc {
+  int m, n;
+  double* X; int ldx;
+  double* W; int ldw;
+  double* sigma;    // n
+  int* perm;        // n
+  int* info;        // optional: sweeps used (negative if the sweep cap was hit)
+};
+void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, cudaStream_t s,
+                   int* d_flags);
+
+// ---- truncation rule (tt_kernels.cu): floor(s, tol) then min(k, rmax, #(s>0))
+struct TruncDesc {
+  const double* sigma;  // unsorted singular values
+  const int* perm;      // order by decreasing sigma
+  int n;                // number of singular values
+  int* rank_out;        // where k is written (device rank array slot)
+};
+void launch_truncate(const TruncDesc* d, int count, double tol, long long rmax, cudaStream_t s);
+
+// Build Ut (rows x cols, ld) with Ut[:, i] = X[:, perm[i]] / sigma[perm[i]] for i < k and
+// 0 for i >= k (k read from *rank); with `unit_w` the columns are taken from W unscaled.
+struct SelectDesc {
+  const double* X; int ldx;  // source columns
+  const double* sigma; const int* perm; const int* rank;
+  int rows, cols;            // output rows and column capacity
+  int src_cols;              // columns of X (perm entries are < src_cols)
+  double* U; int ldu;
+  int scale;                 // 1: divide by sigma; 0: copy; 2: multiply by sigma
+};
+void launch_select(const SelectDesc* d, int count, int max_rows, int max_cols, cudaStream_t s);
+
+// ---- general strided copy / permute of up to 4-D tensors (tt_kernels.cu)
+// dst[i0*ds0 + i1*ds1 + i2*ds2 + i3*ds3] = alpha * src[i0*ss0 + ...] for i < ext.
+struct CopyDesc {
+  const double* src; double* dst;
+  long long ext[4];
+  long long ss[4];
+  long long ds[4];
+  double alpha;
+};
+void launch_copy(const CopyDesc* d, int count, long long max_elems, cudaStream_t s);
+
+// Zero a set of flat ranges.
+struct ZeroDesc { double* p; long long n; };
+void launch_zero(const ZeroDesc* d, int count, long long max_n, cudaStream_t s);
+
+// Sum of squares of `n` doubles per problem, written to out[i] (FP64, deterministic order).
+struct NormDesc { const double* p; long long n; double* out; };
+void launch_sumsq(const NormDesc* d, int count, cudaStream_t s);
+
+// ---- MPO x TT apply (tt_kernels.cu), src/tt_operations.jl:170-194, internal layouts.
+struct ApplyDesc {
+  const double* H;   // internal MPO core (R, n_out, n_in, R')  col-major
+  const double* V;   // internal TT core  (r, n_in, r')         col-major
+  double* Y;         // internal TT core  ((R r), n_out, (R' r')) col-major, R index fastest
+  int R, Rn, r, rn, n;
+};
+void launch_apply(const ApplyDesc* d, int count, long long max_elems, cudaStream_t s);
+
+// ---- Philox sketch generation (tt_kernels.cu): Gaussian block entries
+// dst (Julia layout of the block, flat index e) = scale * N(0,1)_{seed, stream, e}.
+struct PhiloxDesc { double* dst; long long count; unsigned long long seed; unsigned stream; double scale; };
+void launch_philox(const PhiloxDesc* d, int count, long long max_count, cudaStream_t s);
+
+// ---- FP64 -> BF16 conversion and the tcgen05 BF16 GEMM (gemm_bf16_tc.cu)
+struct Bf16GemmDesc {
+  int m, n, k, m0;                // m0: row split (row i = i0 + m0*i1) of the outputs
+  const void* A; long long lda;   // bf16, K-major: A(i, kk) at A[i*lda + kk]
+  const void* B; long long ldb;   // bf16, K-major: B(j, kk) at B[j*ldb + kk]
+  double* C64; float* C32;        // outputs sharing strides: (i0*c_i0 + i1*c_i1 + j*c_j)
+  void* C16;                      // bf16 output with strides (h_i0, h_i1, h_j)
+  long long c_i0, c_i1, c_j, h_i0, h_i1, h_j;
+  double alpha;
+  long long tile_start;
+};
+void launch_gemm_bf16_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags);
+long long bf16_gemm_tiles(const Bf16GemmDesc& d);
+
+}  // namespace ttc

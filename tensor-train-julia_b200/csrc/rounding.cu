@@ -1,0 +1,528 @@
+// Sweep drivers: deterministic TT rounding (src/tt_rounding.jl:146-269) and randomized
+// TT rounding (src/tt_randtools.jl:112-154 with src/sketches.jl:175-305) on device
+// batches.  Internal core layout: column-major (r_{k-1}, n_k, r_k) inside a capacity
+// (cap_{k-1}, n_k, cap_k) slab whose padding is zero, so that
+//   left unfolding  (cap_{k-1} n_k) x cap_k   has ld cap_{k-1} n_k, and
+//   right unfolding  cap_{k-1} x (n_k cap_k)  has ld cap_{k-1}.
+// Every step of a sweep handles all TTs of the batch in one launch per kernel kind.
+#include <algorithm>
+#include <cmath>
+
+#include "builder.cuh"
+#include "drivers.cuh"
+
+namespace ttc {
+
+static inline int qr_tws(int m, int n) { return ((std::min(m, n) + 15) / 16) * 256 + 256; }
+
+// ---------------------------------------------------------------- helpers
+void emit_zero_tts(Builder& B, ttc_batch* y, const std::vector<int>& tts) {
+  std::vector<ZeroDesc> z;
+  for (int t : tts) z.push_back({y->core(t, 0), y->tt_off[t + 1] - y->tt_off[t]});
+  B.zero(z);
+}
+
+void emit_set_ranks(Builder& B, ttc_batch* y, const std::vector<int>& tts, const std::vector<std::vector<int>>& r) {
+  std::vector<SetRankDesc> v;
+  for (size_t i = 0; i < tts.size(); ++i) v.push_back({y->drk(tts[i], 0), B.const_ints(r[i]), y->N + 1});
+  B.setrank(v);
+}
+
+// Copy the TTs of x into y (ranks r), changing only the capacity padding.
+void emit_copy_tts(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<int>& tts,
+                   const std::vector<std::vector<int>>& r) {
+  std::vector<CopyDesc> v;
+  for (size_t i = 0; i < tts.size(); ++i) {
+    const int t = tts[i];
+    for (int k = 0; k < x->N; ++k) {
+      const long long n = x->dims[k], xc = x->capr(t, k), yc = y->capr(t, k);
+      v.push_back(cd3(x->core(t, k), y->core(t, k), r[i][k], n, r[i][k + 1], 1, xc, xc * n, 1, yc, yc * n));
+    }
+  }
+  B.copy(v);
+}
+
+// L->R Householder QR sweep, orthogonalize(x; i=N) (src/tt_rounding.jl:72-79, :92-95).
+// rp[i] are the output ranks (min(n r'_k, r_{k+1}) recursion).
+void emit_orth_left(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<int>& tts,
+                    const std::vector<std::vector<int>>& rp) {
+  const int N = x->N;
+  const size_t T = tts.size();
+  if (T == 0) return;
+  const size_t mark0 = B.mark();
+  std::vector<double*> FR(T), FRn(T);
+  for (size_t i = 0; i < T; ++i) {
+    const int t = tts[i];
+    size_t mx = 1;
+    for (int k = 1; k < N; ++k) mx = std::max(mx, (size_t)rp[i][k] * x->rk(t, k));
+    FR[i] = B.wd(mx);
+    FRn[i] = B.wd(mx);
+  }
+  for (int j = 0; j + 1 < N; ++j) {
+    const size_t m = B.mark();
+    std::vector<GemmDesc> g;
+    std::vector<QRDesc> q;
+    std::vector<CopyDesc> cp;
+    const int n = (int)x->dims[j];
+    for (size_t i = 0; i < T; ++i) {
+      const int t = tts[i];
+      const int a = rp[i][j], an = rp[i][j + 1];
+      const int xr0 = x->rk(t, j), xr1 = x->rk(t, j + 1), xc = x->capr(t, j), yc = y->capr(t, j);
+      double* C = B.wd((size_t)a * n * xr1);
+      double* Q = B.wd((size_t)a * n * an);
+      double* Tws = B.wd(qr_tws(a * n, xr1));
+      const double* A = (j == 0) ? B.ctx->d_one : FR[i];
+      g.push_back(gd(a, n * xr1, xr0, A, 1, a, x->core(t, j), 1, xc, C, 1, a));
+      q.push_back({a * n, xr1, C, a * n, Q, a * n, FRn[i], an, Tws});
+      cp.push_back(cd3(Q, y->core(t, j), a, n, an, 1, a, (long long)a * n, 1, yc, (long long)yc * n));
+    }
+    B.gemm(g);
+    B.qr(q);
+    B.copy(cp);
+    std::swap(FR, FRn);
+    B.release(m);
+  }
+  std::vector<GemmDesc> g;
+  const int n = (int)x->dims[N - 1];
+  for (size_t i = 0; i < T; ++i) {
+    const int t = tts[i];
+    const int a = rp[i][N - 1];
+    const double* A = (N == 1) ? B.ctx->d_one : FR[i];
+    g.push_back(gd(a, n, x->rk(t, N - 1), A, 1, a, x->core(t, N - 1), 1, x->capr(t, N - 1), y->core(t, N - 1), 1,
+                   y->capr(t, N - 1)));
+  }
+  B.gemm(g);
+  B.release(mark0);
+}
+
+// R->L truncated-SVD sweep of _tt_rounding, direction=:left (src/tt_rounding.jl:179-217),
+// on y (left-orthogonal, ranks rp).  The truncation rank of bond j is written to y's
+// device rank array; cores keep their capacity and are zero beyond the kept rank.
+void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const std::vector<std::vector<int>>& rp,
+                   double tol, long long rmax) {
+  const int N = y->N;
+  const size_t T = tts.size();
+  if (T == 0) return;
+  for (int j = N - 1; j >= 1; --j) {
+    const size_t mk = B.mark();
+    std::vector<CopyDesc> cpX, cpY, cpR, cpW, cpT2;
+    std::vector<QRDesc> qr, qr2;
+    std::vector<JacobiDesc> jac;
+    std::vector<TruncDesc> tr;
+    std::vector<SelectDesc> sel;
+    std::vector<GemmDesc> g1, g2, g3;
+    const int n = (int)y->dims[j], nl = (int)y->dims[j - 1];
+    for (size_t i = 0; i < T; ++i) {
+      const int t = tts[i];
+      const int q = rp[i][j], p = n * rp[i][j + 1];
+      const int yc = y->capr(t, j), ycl = y->capr(t, j - 1);
+      const int ml = ycl * nl;
+      int* rank = y->drk(t, j);
+      double* X = B.wd((size_t)p * q);
+      double* T1 = B.wd((size_t)q * q);
+      double* T2 = B.wd((size_t)ml * q);
+      if (p >= q) {
+        // M^T = Q R1 (Householder), R1^T = Q2 R2, one-sided Jacobi on R2^T = R1 Q2: same left
+        // singular vectors as R1 in about half the sweeps (QR-LQ preconditioning); the factor
+        // absorbed into core j-1 stays R1^T U.
+        double* Q = B.wd((size_t)p * q);
+        double* R = B.wd((size_t)q * q);
+        double* Y = B.wd((size_t)q * q);
+        double* R2 = B.wd((size_t)q * q);
+        double* Rc = B.wd((size_t)q * q);
+        double* sig = B.wd(q);
+        int* perm = B.wi(q);
+        double* Tws = B.wd(qr_tws(p, q));
+        double* Tws2 = B.wd(qr_tws(q, q));
+        double* Ut = B.wd((size_t)q * q);
+        cpX.push_back(cd2(y->core(t, j), X, q, p, 1, yc, p, 1));
+        qr.push_back({p, q, X, p, Q, p, R, q, Tws});
+        cpY.push_back(cd2(R, Y, q, q, 1, q, q, 1));
+        qr2.push_back({q, q, Y, q, nullptr, 0, R2, q, Tws2});
+        cpR.push_back(cd2(R2, Rc, q, q, 1, q, q, 1));
+        jac.push_back({q, q, Rc, q, nullptr, 0, sig, perm});
+        tr.push_back({sig, perm, q, rank});
+        sel.push_back({Rc, q, sig, perm, rank, q, q, q, Ut, q, 1});
+        g1.push_back(gd(p, q, q, Q, 1, p, Ut, 1, q, y->core(t, j), yc, 1));
+        g2.push_back(gd(q, q, q, R, q, 1, Ut, 1, q, T1, 1, q));
+      } else {
+        double* Q = B.wd((size_t)q * p);
+        double* R = B.wd((size_t)p * p);
+        double* Rc = B.wd((size_t)p * p);
+        double* W = B.wd((size_t)p * p);
+        double* sig = B.wd(p);
+        int* perm = B.wi(p);
+        double* Tws = B.wd(qr_tws(q, p));
+        double* Wt = B.wd((size_t)p * q);
+        double* Bt = B.wd((size_t)p * q);
+        cpX.push_back(cd2(y->core(t, j), X, q, p, 1, yc, 1, q));
+        qr.push_back({q, p, X, q, Q, q, R, p, Tws});
+        cpR.push_back(cd2(R, Rc, p, p, 1, p, 1, p));
+        jac.push_back({p, p, Rc, p, W, p, sig, perm});
+        tr.push_back({sig, perm, p, rank});
+        sel.push_back({W, p, sig, perm, rank, p, q, p, Wt, p, 0});
+        sel.push_back({Rc, p, sig, perm, rank, p, q, p, Bt, p, 0});
+        cpW.push_back(cd2(Wt, y->core(t, j), p, q, 1, p, yc, 1));
+        g2.push_back(gd(q, q, p, Q, 1, q, Bt, 1, p, T1, 1, q));
+      }
+      g3.push_back(gd(ml, q, q, y->core(t, j - 1), 1, ml, T1, 1, q, T2, 1, ml));
+      cpT2.push_back(cd2(T2, y->core(t, j - 1), ml, q, 1, ml, 1, ml));
+    }
+    B.copy(cpX);
+    B.qr(qr);
+    B.copy(cpY);
+    B.qr(qr2);
+    B.copy(cpR);
+    B.jacobi(jac);
+    B.trunc(tr, tol, rmax);
+    B.select(sel);
+    B.gemm(g1);
+    B.copy(cpW);
+    B.gemm(g2);
+    B.gemm(g3);
+    B.copy(cpT2);
+    B.release(mk);
+  }
+}
+
+// Early exit of _tt_rounding (src/tt_rounding.jl:179-181): norm(core N) < tol.
+void emit_zero_check(Builder& B, ttc_batch* y, const std::vector<int>& tts, int core, double tol) {
+  std::vector<NormDesc> nd;
+  std::vector<ZeroChkDesc> zc;
+  for (int t : tts) {
+    double* s = B.wd(1);
+    const int k = core;
+    nd.push_back({y->core(t, k), (long long)y->capr(t, k) * y->dims[k] * y->capr(t, k + 1), s});
+    zc.push_back({s, y->d_zero + t, tol});
+  }
+  B.sumsq(nd);
+  B.zerochk(zc);
+}
+
+void emit_finalize(Builder& B, ttc_batch* y, const std::vector<int>& tts, const std::vector<std::vector<int>>& rp) {
+  std::vector<FinalDesc> v;
+  for (size_t i = 0; i < tts.size(); ++i) {
+    const int t = tts[i];
+    v.push_back({y->d_zero + t, y->core(t, 0), y->tt_off[t + 1] - y->tt_off[t], y->drk(t, 0), B.const_ints(rp[i]),
+                 y->N + 1});
+  }
+  B.finalize(v);
+}
+
+std::vector<int> orth_left_ranks(const ttc_batch* x, int t) {
+  const int N = x->N;
+  std::vector<int> r(N + 1, 1);
+  for (int k = 0; k + 1 < N; ++k) r[k + 1] = (int)std::min<long long>((long long)x->dims[k] * r[k], x->rk(t, k + 1));
+  r[N] = 1;
+  return r;
+}
+
+bool is_left_orth(const ttc_batch* x, int t) {
+  for (int k = 0; k + 1 < x->N; ++k)
+    if (x->h_ot[(size_t)t * x->N + k] != 1) return false;
+  return true;
+}
+
+// ---------------------------------------------------------------- deterministic rounding
+void round_det(ttc_context* c, ttc_batch* x, const ttc_round_opts& o, ttc_batch* y) {
+  TTC_REQUIRE(o.direction == TTC_DIR_LEFT || o.direction == TTC_DIR_RIGHT, TTC_EARG,
+              "Invalid direction. Use direction=:right or direction=:left");
+  TTC_REQUIRE(o.direction == TTC_DIR_LEFT, TTC_EARG, "direction=:right is served by the host wrapper (reversal)");
+  TTC_REQUIRE(x != y, TTC_EARG, "round: input and output batches must differ");
+  TTC_REQUIRE(y->count == x->count && y->N == x->N && y->dims == x->dims, TTC_EDIM, "round: output batch shape differs");
+  batch_sync_ranks(x);
+  const int N = x->N;
+  std::vector<int> all, orth, keep;
+  std::vector<std::vector<int>> rp_all, rp_orth, rp_keep;
+  for (int t = 0; t < x->count; ++t) {
+    all.push_back(t);
+    std::vector<int> r;
+    if (is_left_orth(x, t)) {
+      r.assign(x->h_rks.begin() + (size_t)t * (N + 1), x->h_rks.begin() + (size_t)(t + 1) * (N + 1));
+      keep.push_back(t);
+      rp_keep.push_back(r);
+    } else {
+      r = orth_left_ranks(x, t);
+      orth.push_back(t);
+      rp_orth.push_back(r);
+    }
+    for (int k = 0; k <= N; ++k)
+      TTC_REQUIRE(y->capr(t, k) >= r[k], TTC_EDIM, "round: output capacity below the orthogonalised ranks");
+    rp_all.push_back(r);
+  }
+  char kb[128];
+  snprintf(kb, sizeof kb, "det:%.17g:%lld:", o.tol, (long long)o.rmax);
+  const std::string key = std::string(kb) + batch_key(x) + batch_key(y);
+  Plan* p = get_plan(c, key, [&](Builder& B) {
+    B.stage(0);
+    emit_zero_tts(B, y, all);
+    emit_set_ranks(B, y, all, rp_all);
+    emit_copy_tts(B, x, y, keep, rp_keep);
+    emit_orth_left(B, x, y, orth, rp_orth);
+    B.stage(1);
+    emit_zero_check(B, y, all, N - 1, o.tol);
+    emit_svd_left(B, y, all, rp_all, o.tol, o.rmax);
+    emit_finalize(B, y, all, rp_all);
+    B.stage(2);
+  });
+  run_plan(c, *p);
+  for (int t = 0; t < y->count; ++t)
+    for (int k = 0; k < N; ++k) y->h_ot[(size_t)t * N + k] = (k == 0) ? 0 : -1;
+  for (int t = 0; t < y->count; ++t)
+    for (int k = 0; k <= N; ++k) y->h_rks[(size_t)t * (N + 1) + k] = rp_all[t][k];
+  y->rks_dirty = true;
+  y->version++;
+}
+
+// ---------------------------------------------------------------- reverse sketch
+// Sketch blocks of the reverse recursive sketch (src/sketches.jl:44-84, :186-198).
+SketchPlan sketch_plan(const std::vector<long long>& dims, const std::vector<long long>& rks, long long block_rks) {
+  const int N = (int)dims.size();
+  SketchPlan sp;
+  sp.b.assign(N + 1, 1);
+  for (int k = 0; k < N; ++k) sp.b[k] = block_rks <= 0 ? N : (int)block_rks;
+  sp.b[N] = 1;
+  for (int k = N - 1; k >= 0; --k) sp.b[k] = (int)std::min<long long>(sp.b[k], dims[k] * sp.b[k + 1]);
+  sp.p.assign(N + 1, 1);
+  for (int k = 0; k <= N; ++k) sp.p[k] = (int)((rks[k] + sp.b[k] - 1) / sp.b[k]);
+  for (int i = 1; i < N; ++i) sp.p[i] = std::max(sp.p[i], sp.p[i - 1]);
+  sp.p[N] = 1;
+  sp.s.resize(N + 1);
+  for (int k = 0; k <= N; ++k) sp.s[k] = sp.b[k] * sp.p[k];
+  return sp;
+}
+
+// Emit generation of the raw sketch blocks (Julia layout (b_{k+1}, n, b_k, p_k)) into raw[k]
+// and their permutation into the GEMM layout (n, b_{k+1}, b_k, p_k) in S[k].
+void emit_sketch_blocks(Builder& B, const std::vector<long long>& dims, const SketchPlan& sp, const ttc_sketch_opts& o,
+                        const std::vector<const double*>& host_raw, std::vector<double*>& S) {
+  const int N = (int)dims.size();
+  S.assign(N, nullptr);
+  std::vector<double*> raw(N, nullptr);
+  std::vector<PhiloxDesc> ph;
+  std::vector<QRDesc> qr;
+  std::vector<CopyDesc> cpQ, cpS;
+  std::vector<ZeroDesc> zr;
+  for (int k = 0; k < N; ++k) {
+    const long long bl = sp.b[k + 1], n = dims[k], br = sp.b[k], pk = sp.p[k];
+    const long long cnt = bl * n * br * pk;
+    S[k] = B.wd(cnt);
+    if (!host_raw.empty()) { raw[k] = const_cast<double*>(host_raw[k]); continue; }
+    raw[k] = B.wd(cnt);
+    const bool orth = o.orthogonal != 0;
+    const bool ident = orth && (br == bl * n);
+    if (ident) {
+      // identity 'sketch' (src/sketches.jl:58-65): block[i,i,j] = 1
+      zr.push_back({raw[k], cnt});
+      CopyDesc c{};   // write ones on the diagonal: src = the device constant 1.0 with zero strides
+      c.src = B.ctx->d_one; c.dst = raw[k];
+      c.ext[0] = br; c.ext[1] = pk; c.ext[2] = 1; c.ext[3] = 1;
+      c.ss[0] = 0; c.ss[1] = 0;
+      c.ds[0] = bl * n + 1; c.ds[1] = bl * n * br;
+      c.alpha = 1.0;
+      cpQ.push_back(c);
+      continue;
+    }
+    const double scale = orth ? 1.0 : 1.0 / std::sqrt((double)br);
+    ph.push_back({raw[k], cnt, (unsigned long long)o.seed, (unsigned)k, scale});
+    if (orth) {
+      // QR of each (bl*n x br) block, Q scaled by sqrt(bl*n/br) (src/sketches.jl:71-78)
+      for (long long j = 0; j < pk; ++j) {
+        double* A = raw[k] + j * bl * n * br;
+        double* Qd = B.wd(bl * n * br);
+        double* Tws = B.wd(qr_tws((int)(bl * n), (int)br));
+        qr.push_back({(int)(bl * n), (int)br, A, (int)(bl * n), Qd, (int)(bl * n), nullptr, 0, Tws});
+        cpQ.push_back(cd2(Qd, A, bl * n, br, 1, bl * n, 1, bl * n, std::sqrt((double)(bl * n) / (double)br)));
+      }
+    }
+  }
+  B.philox(ph);
+  B.zero(zr);
+  B.qr(qr);
+  B.copy(cpQ);
+  for (int k = 0; k < N; ++k) {
+    const long long bl = sp.b[k + 1], n = dims[k], br = sp.b[k], pk = sp.p[k];
+    // raw (be, z, b, j) at be + bl*(z + n*(b + br*j))  ->  S (z, be, (b, j)) at z + n*be + n*bl*(b + br*j)
+    cpS.push_back(cd3(raw[k], S[k], bl, n, br * pk, 1, bl, bl * n, n, 1, n * bl));
+  }
+  B.copy(cpS);
+}
+
+// Reverse recursive sketch of every TT of x (src/sketches.jl:221-239) in FP64.  W[t][k] is
+// the unscaled (r_k, b_k, p_k) array; the 1/sqrt(p_k) factor (src/sketches.jl:300-302) is
+// applied by the consumers.  W[t][N] is the constant 1.
+void emit_sketch_f64(Builder& B, ttc_batch* x, const std::vector<int>& tts, const SketchPlan& sp,
+                     const std::vector<double*>& S, std::vector<std::vector<double*>>& W) {
+  const int N = x->N;
+  W.assign(tts.size(), std::vector<double*>(N + 1, nullptr));
+  for (size_t i = 0; i < tts.size(); ++i) {
+    const int t = tts[i];
+    for (int k = 0; k < N; ++k) W[i][k] = B.wd((size_t)x->rk(t, k) * sp.b[k] * sp.p[k]);
+    W[i][N] = B.ctx->d_one;
+  }
+  for (int k = N - 1; k >= 0; --k) {
+    const size_t mk = B.mark();
+    std::vector<GemmDesc> g1, g2;
+    const int n = (int)x->dims[k];
+    const int bl = sp.b[k + 1], br = sp.b[k], pk = sp.p[k];
+    for (size_t i = 0; i < tts.size(); ++i) {
+      const int t = tts[i];
+      const int r0 = x->rk(t, k), r1 = x->rk(t, k + 1), xc = x->capr(t, k);
+      double* Tm = B.wd((size_t)r0 * n * bl * pk);
+      // T[(a,z), be] = sum_al A_k[a, z, al] W_{k+1}[al, be, j]
+      GemmDesc d = gd(r0 * n, bl, r1, x->core(t, k), 1, (long long)xc * n, W[i][k + 1], 1, r1, Tm, 1,
+                      (long long)r0 * n);
+      d.m0 = r0; d.a_i0 = 1; d.a_i1 = xc;                       // rows a + r0*z inside the capacity slab
+      d.c_i0 = 1; d.c_i1 = r0;                                  // packed rows of T
+      d.batch = pk;
+      d.a_b = 0;
+      d.b_b = (k < N - 1) ? (long long)r1 * bl : 0;
+      d.c_b = (long long)r0 * n * bl;
+      g1.push_back(d);
+      // W_k[a, b, j] = sum_{z, be} T[a, z, be] S[z, be, b, j]
+      GemmDesc e = gd(r0, br, n * bl, Tm, 1, r0, S[k], 1, (long long)n * bl, W[i][k], 1, r0);
+      e.batch = pk;
+      e.a_b = (long long)r0 * n * bl;
+      e.b_b = (long long)n * bl * br;
+      e.c_b = (long long)r0 * br;
+      g2.push_back(e);
+    }
+    B.gemm(g1);
+    B.gemm(g2);
+    B.release(mk);
+  }
+}
+
+// Left-to-right orthogonalise-and-project sweep of ttrand_rounding
+// (src/tt_randtools.jl:123-151) for single TTs: Z = y_k W_{k+1}, Q = qr(Z), y_{k+1} = Q^T y_k A_{k+1}.
+void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<int>& tts, const SketchPlan& sp,
+                     const std::vector<std::vector<double*>>& W, const std::vector<std::vector<int>>& rho) {
+  const int N = x->N;
+  const size_t T = tts.size();
+  std::vector<double*> Y(T), Yn(T);
+  std::vector<int> yld(T);
+  const size_t mark0 = B.mark();
+  for (size_t i = 0; i < T; ++i) {
+    const int t = tts[i];
+    size_t mx = 1;
+    for (int k = 1; k < N; ++k) mx = std::max(mx, (size_t)((long long)rho[i][k] * x->dims[k] * x->rk(t, k + 1)));
+    Y[i] = B.wd(mx);
+    Yn[i] = B.wd(mx);
+  }
+  for (int k = 0; k + 1 < N; ++k) {
+    const size_t mk = B.mark();
+    std::vector<GemmDesc> gz, gp, gy;
+    std::vector<QRDesc> qr;
+    std::vector<CopyDesc> cp;
+    const int n = (int)x->dims[k], nn = (int)x->dims[k + 1];
+    const int s = sp.s[k + 1];
+    const double wscale = 1.0 / std::sqrt((double)sp.p[k + 1]);
+    for (size_t i = 0; i < T; ++i) {
+      const int t = tts[i];
+      const int rh = rho[i][k], rhn = rho[i][k + 1], r1 = x->rk(t, k + 1), r2 = x->rk(t, k + 2);
+      // y_k: (rh, n, r1); for k = 0 it is core 0 of x (cap_0 = 1)
+      const double* Yk = (k == 0) ? x->core(t, 0) : Y[i];
+      const long long yk_ld = (k == 0) ? (long long)x->capr(t, 0) * n : (long long)rh * n;
+      double* Z = B.wd((size_t)rh * n * s);
+      double* Q = B.wd((size_t)rh * n * rhn);
+      double* P = B.wd((size_t)rhn * r1);
+      double* Tws = B.wd(qr_tws(rh * n, s));
+      gz.push_back(gd(rh * n, s, r1, Yk, 1, yk_ld, W[i][k + 1], 1, r1, Z, 1, (long long)rh * n, wscale));
+      qr.push_back({rh * n, s, Z, rh * n, Q, rh * n, nullptr, 0, Tws});
+      const int yc = y->capr(t, k);
+      cp.push_back(cd3(Q, y->core(t, k), rh, n, rhn, 1, rh, (long long)rh * n, 1, yc, (long long)yc * n));
+      gp.push_back(gd(rhn, r1, rh * n, Q, (long long)rh * n, 1, Yk, 1, yk_ld, P, 1, rhn));
+      gy.push_back(gd(rhn, nn * r2, r1, P, 1, rhn, x->core(t, k + 1), 1, x->capr(t, k + 1), Yn[i], 1, rhn));
+    }
+    B.gemm(gz);
+    B.qr(qr);
+    B.copy(cp);
+    B.gemm(gp);
+    B.gemm(gy);
+    std::swap(Y, Yn);
+    B.release(mk);
+  }
+  std::vector<CopyDesc> cp;
+  for (size_t i = 0; i < T; ++i) {
+    const int t = tts[i];
+    const int rh = rho[i][N - 1], n = (int)x->dims[N - 1], yc = y->capr(t, N - 1);
+    const double* src = (N == 1) ? x->core(t, 0) : Y[i];
+    cp.push_back(cd2(src, y->core(t, N - 1), rh, n, 1, rh, 1, yc));
+  }
+  B.copy(cp);
+  B.release(mark0);
+}
+
+std::vector<int> rand_out_ranks(const std::vector<long long>& dims, const SketchPlan& sp) {
+  const int N = (int)dims.size();
+  std::vector<int> r(N + 1, 1);
+  for (int k = 0; k + 1 < N; ++k) r[k + 1] = (int)std::min<long long>(dims[k] * r[k], sp.s[k + 1]);
+  r[N] = 1;
+  return r;
+}
+
+void round_rand(ttc_context* c, ttc_batch* x, const std::vector<long long>& rks, const ttc_sketch_opts& o,
+                const ttc_round_opts* after, ttc_batch* y, const std::vector<const double*>& host_raw,
+                const std::string& raw_key) {
+  TTC_REQUIRE(x != y, TTC_EARG, "round: input and output batches must differ");
+  TTC_REQUIRE(y->count == x->count && y->N == x->N && y->dims == x->dims, TTC_EDIM, "round: output batch shape differs");
+  const int N = x->N;
+  TTC_REQUIRE((int)rks.size() == N + 1, TTC_EDIM, "ttrand_rounding: rks must have length N+1");
+  TTC_REQUIRE(rks[N] == 1, TTC_EDIM, "ttrand_rounding: rks[N+1] must be 1");
+  TTC_REQUIRE(!o.orthogonal || o.block_rks > 0 || true, TTC_EARG, "");
+  batch_sync_ranks(x);
+  for (int t = 0; t < x->count; ++t)
+    TTC_REQUIRE(x->rk(t, N) == 1, TTC_EDIM, "ttrand_rounding: the last TT rank must be 1");
+  const SketchPlan sp = sketch_plan(x->dims, rks, o.block_rks);
+  if (o.orthogonal)
+    for (int k = 0; k < N; ++k)
+      TTC_REQUIRE(sp.b[k] <= (long long)x->dims[k] * sp.b[k + 1], TTC_EARG, "generate_sketch_blocks: right_rank > dim*left_rank");
+  const std::vector<int> rho = rand_out_ranks(x->dims, sp);
+  std::vector<int> all;
+  std::vector<std::vector<int>> rho_all;
+  for (int t = 0; t < x->count; ++t) {
+    all.push_back(t);
+    rho_all.push_back(rho);
+    for (int k = 0; k <= N; ++k)
+      TTC_REQUIRE(y->capr(t, k) >= rho[k], TTC_EDIM, "ttrand_rounding: output capacity below the sketch ranks");
+  }
+  char kb[256];
+  snprintf(kb, sizeof kb, "rand:%d:%llu:%lld:%d:%d:%.17g:%lld:", o.orthogonal, (unsigned long long)o.seed,
+           (long long)o.block_rks, o.precision, after ? 1 : 0, after ? after->tol : 0.0, after ? (long long)after->rmax : 0LL);
+  std::string key = std::string(kb) + raw_key + batch_key(x) + batch_key(y);
+  for (long long r : rks) key += std::to_string(r) + ",";
+  Plan* p = get_plan(c, key, [&](Builder& B) {
+    B.stage(0);
+    emit_zero_tts(B, y, all);
+    emit_set_ranks(B, y, all, rho_all);
+    std::vector<double*> S;
+    emit_sketch_blocks(B, x->dims, sp, o, host_raw, S);
+    std::vector<std::vector<double*>> W;
+    if (o.precision == TTC_PREC_BF16) emit_sketch_bf16(B, x, all, sp, S, W);
+    else emit_sketch_f64(B, x, all, sp, S, W);
+    B.stage(1);
+    emit_rand_sweep(B, x, y, all, sp, W, rho_all);
+    B.stage(2);
+    if (after) {
+      emit_zero_check(B, y, all, N - 1, after->tol);
+      emit_svd_left(B, y, all, rho_all, after->tol, after->rmax);
+      emit_finalize(B, y, all, rho_all);
+    }
+    B.stage(3);
+  });
+  run_plan(c, *p);
+  for (int t = 0; t < y->count; ++t) {
+    for (int k = 0; k < N; ++k) {
+      int ot;
+      if (after) ot = (k == 0) ? 0 : -1;
+      else ot = (k < N - 1) ? 1 : 0;
+      y->h_ot[(size_t)t * N + k] = ot;
+    }
+    for (int k = 0; k <= N; ++k) y->h_rks[(size_t)t * (N + 1) + k] = rho[k];
+  }
+  y->rks_dirty = after != nullptr;
+  if (after) for (int t = 0; t < y->count; ++t) {}
+  y->version++;
+}
+
+}  // namespace ttc

@@ -1,0 +1,136 @@
+// Kernel-level test entry points: run one device kernel on host arrays so the tests can
+// check it against numpy in isolation.  They are exported for the test suite only and are
+// not part of the public ABI in include/ttcuda.h.
+#include <cstring>
+
+#include "api_impl.cuh"
+#include "regions.cuh"
+
+using namespace ttc;
+
+namespace {
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  explicit DevBuf(size_t bytes) : n(bytes) {
+    if (bytes == 0) bytes = 8;
+    TTC_CUDA(cudaMalloc(&p, bytes));
+    TTC_CUDA(cudaMemset(p, 0, bytes));
+    region_add(p, bytes);
+  }
+  ~DevBuf() { region_remove(p); cudaFree(p); }
+  template <class T> T* as() const { return (T*)p; }
+};
+
+template <class F>
+int hook(ttc_context* c, F&& f) {
+  try {
+    TTC_CUDA(cudaSetDevice(c->device));
+    f();
+    TTC_CUDA(cudaStreamSynchronize(c->stream));
+    check_device_flags(c);
+    return TTC_OK;
+  } catch (const Error& e) {
+    c->err = e.what();
+    return e.status;
+  } catch (const std::exception& e) {
+    c->err = e.what();
+    return TTC_EINTERNAL;
+  }
+}
+
+void run_plan_once(ttc_context* c, const std::function<void(Builder&)>& fn) {
+  static unsigned long long serial = 0;
+  const std::string key = "hook:" + std::to_string(++serial);
+  Plan* p = get_plan(c, key, fn);
+  run_plan(c, *p);
+  TTC_CUDA(cudaStreamSynchronize(c->stream));
+  c->plans.erase(key);
+}
+}  // namespace
+
+extern "C" {
+
+// C = alpha * A * B + beta * C with split strides (a_str = {i0, i1, k0, k1, b}, ...).
+int ttc_test_gemm(ttc_context* c, int m, int n, int k, int batch, int m0, int n0, int k0e, const double* A,
+                  long long a_len, const long long* as, const double* Bh, long long b_len, const long long* bs,
+                  double* Ch, long long c_len, const long long* cs, double alpha, double beta) {
+  return hook(c, [&] {
+    DevBuf dA(a_len * 8), dB(b_len * 8), dC(c_len * 8);
+    TTC_CUDA(cudaMemcpy(dA.p, A, a_len * 8, cudaMemcpyHostToDevice));
+    TTC_CUDA(cudaMemcpy(dB.p, Bh, b_len * 8, cudaMemcpyHostToDevice));
+    TTC_CUDA(cudaMemcpy(dC.p, Ch, c_len * 8, cudaMemcpyHostToDevice));
+    run_plan_once(c, [&](Builder& B) {
+      GemmDesc d{};
+      d.m = m; d.n = n; d.k = k; d.batch = batch; d.m0 = m0; d.n0 = n0; d.k0e = k0e;
+      d.A = dA.as<double>(); d.a_i0 = as[0]; d.a_i1 = as[1]; d.a_k0 = as[2]; d.a_k1 = as[3]; d.a_b = as[4];
+      d.B = dB.as<double>(); d.b_k0 = bs[0]; d.b_k1 = bs[1]; d.b_j0 = bs[2]; d.b_j1 = bs[3]; d.b_b = bs[4];
+      d.C = dC.as<double>(); d.c_i0 = cs[0]; d.c_i1 = cs[1]; d.c_j0 = cs[2]; d.c_j1 = cs[3]; d.c_b = cs[4];
+      d.alpha = alpha; d.beta = beta;
+      B.gemm({d});
+    });
+    TTC_CUDA(cudaMemcpy(Ch, dC.p, c_len * 8, cudaMemcpyDeviceToHost));
+  });
+}
+
+// Householder QR of A (m x n, col-major): Q (m x K), R (K x n).
+int ttc_test_qr(ttc_context* c, int m, int n, const double* A, double* Q, double* R) {
+  return hook(c, [&] {
+    const int K = std::min(m, n);
+    DevBuf dA((size_t)m * n * 8), dQ((size_t)m * K * 8), dR((size_t)K * n * 8), dT((size_t)((K + 15) / 16 + 1) * 256 * 8);
+    TTC_CUDA(cudaMemcpy(dA.p, A, (size_t)m * n * 8, cudaMemcpyHostToDevice));
+    run_plan_once(c, [&](Builder& B) {
+      B.qr({{m, n, dA.as<double>(), m, dQ.as<double>(), m, dR.as<double>(), K, dT.as<double>()}});
+    });
+    TTC_CUDA(cudaMemcpy(Q, dQ.p, (size_t)m * K * 8, cudaMemcpyDeviceToHost));
+    TTC_CUDA(cudaMemcpy(R, dR.p, (size_t)K * n * 8, cudaMemcpyDeviceToHost));
+  });
+}
+
+// One-sided Jacobi of X (m x n): X <- X W (orthogonal columns), sigma, perm; W if accw.
+// *sweeps receives the sweeps used (negative when the cap was hit; not raised as an error here).
+int ttc_test_jacobi(ttc_context* c, int m, int n, double* X, int accw, double* W, double* sigma, int* perm,
+                    int* sweeps) {
+  return hook(c, [&] {
+    DevBuf dX((size_t)m * n * 8), dW((size_t)n * n * 8), ds((size_t)n * 8), dp((size_t)n * 4), di(8);
+    TTC_CUDA(cudaMemcpy(dX.p, X, (size_t)m * n * 8, cudaMemcpyHostToDevice));
+    run_plan_once(c, [&](Builder& B) {
+      JacobiDesc d{m, n, dX.as<double>(), m, accw ? dW.as<double>() : nullptr, n, ds.as<double>(), dp.as<int>(),
+                   di.as<int>()};
+      B.jacobi({d});
+    });
+    TTC_CUDA(cudaMemcpy(X, dX.p, (size_t)m * n * 8, cudaMemcpyDeviceToHost));
+    if (accw) TTC_CUDA(cudaMemcpy(W, dW.p, (size_t)n * n * 8, cudaMemcpyDeviceToHost));
+    TTC_CUDA(cudaMemcpy(sigma, ds.p, (size_t)n * 8, cudaMemcpyDeviceToHost));
+    TTC_CUDA(cudaMemcpy(perm, dp.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    TTC_CUDA(cudaMemcpy(sweeps, di.p, 4, cudaMemcpyDeviceToHost));
+    TTC_CUDA(cudaMemset(c->d_flags, 0, sizeof(int)));
+  });
+}
+
+// tcgen05 BF16 GEMM: C (m x n, col-major, FP64 out) = alpha * bf16(A) bf16(B)^T with A (m x k)
+// and B (n x k) given row-major in FP64 (converted to BF16 on the device).
+int ttc_test_bf16_gemm(ttc_context* c, int m, int n, int k, const double* A, const double* Bh, double* C,
+                       double alpha) {
+  return hook(c, [&] {
+    const long long lda = (k + 7) / 8 * 8;
+    DevBuf dA((size_t)m * k * 8), dB((size_t)n * k * 8), dC((size_t)m * n * 8);
+    DevBuf a16((size_t)m * lda * 2 + 64), b16((size_t)n * lda * 2 + 64);
+    TTC_CUDA(cudaMemcpy(dA.p, A, (size_t)m * k * 8, cudaMemcpyHostToDevice));
+    TTC_CUDA(cudaMemcpy(dB.p, Bh, (size_t)n * k * 8, cudaMemcpyHostToDevice));
+    run_plan_once(c, [&](Builder& B) {
+      CvtDesc ca{dA.as<double>(), a16.p, m, k, k, 1, lda, 1, 1.0};
+      CvtDesc cb{dB.as<double>(), b16.p, n, k, k, 1, lda, 1, 1.0};
+      B.cvt_bf16({ca, cb});
+      Bf16GemmDesc d{};
+      d.m = m; d.n = n; d.k = k; d.m0 = std::max(m, 1);
+      d.A = a16.p; d.lda = lda; d.B = b16.p; d.ldb = lda;
+      d.C64 = dC.as<double>(); d.c_i0 = 1; d.c_i1 = 0; d.c_j = m;
+      d.alpha = alpha;
+      B.bf16gemm({d});
+    });
+    TTC_CUDA(cudaMemcpy(C, dC.p, (size_t)m * n * 8, cudaMemcpyDeviceToHost));
+  });
+}
+
+}  // extern "C"

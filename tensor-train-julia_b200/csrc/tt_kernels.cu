@@ -1,0 +1,225 @@
+// Bandwidth-bound helper kernels of libttcuda: strided tensor copies (layout changes
+// between the Julia core layout and the internal one), zero fills, sums of squares,
+// the truncation rule, singular-vector selection, the MPO x TT apply and the Philox
+// sketch generator.  Grids are sized in multiples of the SM count where they stream.
+#include "kernels.cuh"
+
+namespace ttc {
+namespace {
+constexpr int NT = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+}  // namespace
+
+// ---------------------------------------------------------------- strided copy
+__global__ void copy4_kernel(const CopyDesc* __restrict__ descs) {
+  const CopyDesc D = descs[blockIdx.y];
+  const long long e0 = D.ext[0], e1 = D.ext[1], e2 = D.ext[2], e3 = D.ext[3];
+  const long long total = e0 * e1 * e2 * e3;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long r = e;
+    const long long i0 = r % e0; r /= e0;
+    const long long i1 = r % e1; r /= e1;
+    const long long i2 = r % e2; const long long i3 = r / e2;
+    const double v = D.src[i0 * D.ss[0] + i1 * D.ss[1] + i2 * D.ss[2] + i3 * D.ss[3]];
+    D.dst[i0 * D.ds[0] + i1 * D.ds[1] + i2 * D.ds[2] + i3 * D.ds[3]] = D.alpha * v;
+  }
+}
+
+void launch_copy(const CopyDesc* d, int count, long long max_elems, cudaStream_t s) {
+  if (count <= 0 || max_elems <= 0) return;
+  const long long blocks = std::min<long long>((max_elems + NT - 1) / NT, 148LL * 8);
+  dim3 grid((unsigned)blocks, (unsigned)count);
+  copy4_kernel<<<grid, NT, 0, s>>>(d);
+  TTC_CHECK_LAUNCH();
+}
+
+__global__ void zero_kernel(const ZeroDesc* __restrict__ descs) {
+  const ZeroDesc D = descs[blockIdx.y];
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < D.n; e += (long long)gridDim.x * blockDim.x)
+    D.p[e] = 0.0;
+}
+
+void launch_zero(const ZeroDesc* d, int count, long long max_n, cudaStream_t s) {
+  if (count <= 0 || max_n <= 0) return;
+  const long long blocks = std::min<long long>((max_n + NT - 1) / NT, 148LL * 8);
+  zero_kernel<<<dim3((unsigned)blocks, (unsigned)count), NT, 0, s>>>(d);
+  TTC_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------- sum of squares
+__global__ void sumsq_kernel(const NormDesc* __restrict__ descs) {
+  __shared__ double red[NT / 32];
+  const NormDesc D = descs[blockIdx.x];
+  double a = 0.0;
+  for (long long e = threadIdx.x; e < D.n; e += NT) a = fma(D.p[e], D.p[e], a);
+  a = warp_sum(a);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < NT / 32; ++i) s += red[i];
+    *D.out = s;
+  }
+}
+
+void launch_sumsq(const NormDesc* d, int count, cudaStream_t s) {
+  if (count <= 0) return;
+  sumsq_kernel<<<count, NT, 0, s>>>(d);
+  TTC_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------- truncation rule
+// floor(s, tol; degen_tol=1e-5) of src/tt_rounding.jl:297-315 on the sorted values, then
+// k = min(k, rmax, #(s > 0)) (src/tt_rounding.jl:198-199).  One thread per problem: the
+// rule is a short sequential scan in FP64.
+__global__ void truncate_kernel(const TruncDesc* __restrict__ descs, int count, double tol, long long rmax) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= count) return;
+  const TruncDesc D = descs[p];
+  const int d = D.n;
+  int k;
+  if (d <= 0) { k = 0; }
+  else if (tol == 0.0) { k = d; }
+  else {
+    double norm2 = 0.0;
+    for (int i = 0; i < d; ++i) { const double v = D.sigma[D.perm[i]]; norm2 = fma(v, v, norm2); }
+    int i = d;
+    double weight = 0.0;
+    const double thr = tol * tol * norm2;
+    while (i > 0 && weight < thr) {
+      const double v = D.sigma[D.perm[i - 1]];
+      weight = fma(v, v, weight);
+      --i;
+    }
+    ++i;
+    while (i < d) {
+      const double a = D.sigma[D.perm[i - 1]], b = D.sigma[D.perm[i]];
+      const double ratio = b / a;
+      if (isfinite(ratio) && fabs(1.0 - ratio) <= 1e-5) ++i; else break;
+    }
+    k = i;
+  }
+  int npos = 0;
+  for (int i = 0; i < d; ++i) npos += (D.sigma[i] > 0.0);
+  if (k > npos) k = npos;
+  if ((long long)k > rmax) k = (int)rmax;
+  *D.rank_out = k;
+}
+
+void launch_truncate(const TruncDesc* d, int count, double tol, long long rmax, cudaStream_t s) {
+  if (count <= 0) return;
+  truncate_kernel<<<(count + 63) / 64, 64, 0, s>>>(d, count, tol, rmax);
+  TTC_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------- column selection
+__global__ void select_kernel(const SelectDesc* __restrict__ descs) {
+  const SelectDesc D = descs[blockIdx.y];
+  const int k = *D.rank;
+  const long long total = (long long)D.rows * D.cols;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / D.rows), r = (int)(e - (long long)c * D.rows);
+    double v = 0.0;
+    if (c < k) {
+      const int src = D.perm[c];
+      v = D.X[(long long)src * D.ldx + r];
+      if (D.scale == 1) { const double s = D.sigma[src]; v = (s > 0.0) ? v / s : 0.0; }
+      else if (D.scale == 2) v *= D.sigma[src];
+    }
+    D.U[(long long)c * D.ldu + r] = v;
+  }
+}
+
+void launch_select(const SelectDesc* d, int count, int max_rows, int max_cols, cudaStream_t s) {
+  if (count <= 0) return;
+  const long long total = (long long)max_rows * max_cols;
+  const long long blocks = std::max<long long>(1, std::min<long long>((total + NT - 1) / NT, 148LL * 4));
+  select_kernel<<<dim3((unsigned)blocks, (unsigned)count), NT, 0, s>>>(d);
+  TTC_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------- MPO x TT apply
+// Y[(a + R*nu), i, (a' + R'*nu')] = sum_j H[a, i, j, a'] * V[nu, j, nu'] (internal layouts;
+// src/tt_operations.jl:184).  One thread per output element, consecutive threads on the
+// fastest output index a, so H is read coalesced and V is a broadcast.  HBM-bound on Y.
+__global__ void apply_kernel(const ApplyDesc* __restrict__ descs) {
+  const ApplyDesc D = descs[blockIdx.y];
+  const long long Rr = (long long)D.R * D.r, Rrn = (long long)D.Rn * D.rn;
+  const long long total = Rr * D.n * Rrn;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    long long t = e;
+    const int a = (int)(t % D.R); t /= D.R;
+    const int nu = (int)(t % D.r); t /= D.r;
+    const int i = (int)(t % D.n); t /= D.n;
+    const int an = (int)(t % D.Rn); const int nun = (int)(t / D.Rn);
+    double acc = 0.0;
+    for (int j = 0; j < D.n; ++j) {
+      const double h = D.H[a + (long long)D.R * (i + (long long)D.n * (j + (long long)D.n * an))];
+      const double v = D.V[nu + (long long)D.r * (j + (long long)D.n * nun)];
+      acc = fma(h, v, acc);
+    }
+    D.Y[e] = acc;
+  }
+}
+
+void launch_apply(const ApplyDesc* d, int count, long long max_elems, cudaStream_t s) {
+  if (count <= 0 || max_elems <= 0) return;
+  const long long blocks = std::min<long long>((max_elems + NT - 1) / NT, 148LL * 16);
+  apply_kernel<<<dim3((unsigned)blocks, (unsigned)count), NT, 0, s>>>(d);
+  TTC_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------- Philox sketch generator
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC'11): counter (e/4, stream, 0, 0), key (seed lo, seed hi); Box-Muller on the word pairs.
+// The oracle's philox_normals() computes the same sequence on the host.
+__device__ __forceinline__ void philox10(unsigned c[4], unsigned k0, unsigned k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const unsigned long long p0 = 0xD2511F53ull * c[0];
+    const unsigned long long p1 = 0xCD9E8D57ull * c[2];
+    const unsigned hi0 = (unsigned)(p0 >> 32), lo0 = (unsigned)p0;
+    const unsigned hi1 = (unsigned)(p1 >> 32), lo1 = (unsigned)p1;
+    const unsigned n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+    k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+  }
+}
+
+__global__ void philox_kernel(const PhiloxDesc* __restrict__ descs) {
+  const PhiloxDesc D = descs[blockIdx.y];
+  const long long nctr = (D.count + 3) / 4;
+  const double inv = 1.0 / 4294967296.0;
+  const double two_pi = 6.283185307179586476925286766559;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nctr; q += (long long)gridDim.x * blockDim.x) {
+    unsigned c[4] = {(unsigned)q, D.stream, 0u, 0u};
+    philox10(c, (unsigned)D.seed, (unsigned)(D.seed >> 32));
+    const double u0 = (c[0] + 0.5) * inv, u1 = (c[1] + 0.5) * inv;
+    const double u2 = (c[2] + 0.5) * inv, u3 = (c[3] + 0.5) * inv;
+    const double r01 = sqrt(-2.0 * log(u0)), r23 = sqrt(-2.0 * log(u2));
+    double s1, c1, s3, c3;
+    sincos(two_pi * u1, &s1, &c1);
+    sincos(two_pi * u3, &s3, &c3);
+    const double z[4] = {r01 * c1, r01 * s1, r23 * c3, r23 * s3};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const long long e = 4 * q + t;
+      if (e < D.count) D.dst[e] = D.scale * z[t];
+    }
+  }
+}
+
+void launch_philox(const PhiloxDesc* d, int count, long long max_count, cudaStream_t s) {
+  if (count <= 0 || max_count <= 0) return;
+  const long long blocks = std::min<long long>(((max_count + 3) / 4 + NT - 1) / NT, 148LL * 8);
+  philox_kernel<<<dim3((unsigned)blocks, (unsigned)count), NT, 0, s>>>(d);
+  TTC_CHECK_LAUNCH();
+}
+
+}  // namespace ttc
