@@ -1,0 +1,390 @@
+"""Benchmark of the batched TT rounding path (libttcuda on B200).
+
+Workload (the headline configuration): 64 TTvectors, d = 32 sites, n = 2; interior ranks drawn
+uniformly in [16, 256] per TT and bond (seeded, clamped by r_and_d_to_rks); bond-k singular
+values decay like 10^(-i/32) (left-orthonormal random cores, the bond decay absorbed into the
+next core).  Data are synthetic (seeded numpy), generated on the host.
+
+One step rounds the whole batch to tol = 1e-8 in two variants:
+  * mixed : ttrand_rounding with a Gaussian sketch whose contractions run in BF16 on the
+            tcgen05 tensor cores (FP32 accumulation), sketch ranks = default_rank_heuristic
+            (r + ceil(max r / 2)), FP64 range finder / projection, then the FP64 truncated-SVD
+            sweep tt_rounding(tol);                         -> `value`
+  * fp64  : deterministic tt_rounding(tol) (FP64 QR sweep + truncated-SVD sweep) -> `fp64`.
+`value` is whole-job roundings/s with the inputs resident in HBM (device events around K
+replays of the captured plan); `e2e` is the same metric through the C ABI with host buffers
+(upload, round, download every step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tensor-train-julia_b200"))
+
+D, NPHYS, BATCH, RMIN, RMAX, TOL = 32, 2, 64, 16, 256, 1e-8
+METRIC = "TT roundings/s at d=32,r=256: mixed vs FP64 GPU at 1e-8 rel err; % roofline"
+
+
+# ------------------------------------------------------------------------- workload
+def r_and_d(rks, dims, rmax):
+    d = len(dims)
+    new = [1] * len(rks)
+    for i in range(d):
+        new[i] = min(rks[i], int(np.prod(dims[:i])) if i else 1, int(np.prod(dims[i:])), rmax)
+    return new
+
+
+def make_tt(dims, ranks, seed, decay_per=32.0):
+    """Left-orthonormal random cores; the decay 10^(-i/decay_per) of bond k is absorbed into core k+1."""
+    g = np.random.default_rng(seed)
+    N = len(dims)
+    vec, prev = [], np.ones(1)
+    for k in range(N):
+        n, a, b = dims[k], ranks[k], ranks[k + 1]
+        if k < N - 1:
+            # orthonormal columns; a bond wider than n*a (i.i.d. rank draws) gets zero columns,
+            # so its numerical rank is n*a
+            q, _ = np.linalg.qr(g.standard_normal((n * a, b)))
+            q = q[:, :b] if q.shape[1] >= b else np.pad(q, ((0, 0), (0, b - q.shape[1])))
+            core = np.transpose(q.reshape(a, n, b, order="F"), (1, 0, 2)).copy()
+        else:
+            core = g.standard_normal((n, a, b))
+            core /= np.linalg.norm(core)
+        vec.append(np.asfortranarray(core * prev[None, :, None]))
+        # unit RMS keeps the TT norm O(1) over 32 bonds (the zero test of the rounding is absolute)
+        prev = 10.0 ** (-np.arange(b) / decay_per)
+        prev /= np.sqrt(np.mean(prev ** 2))
+    return vec
+
+
+def workload(seed, batch=BATCH):
+    g = np.random.default_rng(seed)
+    dims = (NPHYS,) * D
+    tts = []
+    for i in range(batch):
+        r = [1] + [int(v) for v in g.integers(RMIN, RMAX + 1, size=D - 1)] + [1]
+        r = r_and_d(r, dims, max(r))
+        tts.append((dims, r, make_tt(dims, r, seed * 100003 + i)))
+    return dims, tts
+
+
+def heuristic(rank_lists):
+    """default_rank_heuristic of a list of TTs (src/tt_randtools.jl:40-50)."""
+    rks = list(rank_lists[0])
+    for r in rank_lists[1:]:
+        rks = [max(a, b) for a, b in zip(rks, r)]
+    over = int(math.ceil(0.5 * max(rks)))
+    for k in range(1, len(rks) - 1):
+        rks[k] += over
+    return rks
+
+
+# ------------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, path):
+        self.path, self.proc = path, None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self, device_index):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        try:
+            rows = [l.strip().split(", ") for l in open(self.path) if l.strip()]
+            rows = [r for r in rows if len(r) >= 9 and r[0].strip() == str(device_index)]
+            if not rows:
+                return out
+            sm = [float(r[1]) for r in rows]
+            out["sm_mhz"] = float(np.median(sm))
+            out["sm_max_mhz"] = float(rows[0][2])
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            reasons = set()
+            for r in rows:
+                for nm, v in zip(names, r[5:9]):
+                    if "Active" in v and "Not" not in v:
+                        reasons.add(nm)
+            out["reasons"] = sorted(reasons)
+        except Exception:
+            pass
+        return out
+
+
+# ------------------------------------------------------------------ CPU baselines
+def cpu_reference_rate(dims, tts, rks, sample):
+    """The FP64 CPU restatement of the reference path (ttrand_rounding + tt_rounding, LAPACK via
+    numpy/scipy on all host cores) on `sample` TTs of the batch; returns (roundings/s, seconds)."""
+    sys.path.insert(0, ROOT)
+    from oracle import tt_oracle as o
+    t0 = time.perf_counter()
+    for dims_i, r, vec in tts[:sample]:
+        x = o.TTvector(len(dims_i), [c.copy() for c in vec], tuple(dims_i), list(r), [0] * len(dims_i))
+        y = o.ttrand_rounding(x, rks, orthogonal=False, seed=1234, block_rks=max(rks))
+        o.tt_rounding(y, tol=TOL)
+    dt = time.perf_counter() - t0
+    return sample / dt, dt
+
+
+# ---------------------------------------------------------------------- reference arm
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    dims, tts = workload(seed=7)
+    rks = heuristic([r for _, r, _ in tts])
+    sample = max(1, int(os.environ.get("TTC_REF_SAMPLE", "3")))
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_reference_rate(dims, tts, rks, 1)
+    rates = []
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        r, _ = cpu_reference_rate(dims, tts, rks, sample)
+        rates.append(r)
+    total = time.perf_counter() - t_all
+    v = float(np.mean(rates))
+    cores = os.cpu_count() or 1
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "roundings/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batched rounding: 64 TTs, d=32, n=2, ranks U[16,256], sigma 10^(-i/32), tol 1e-8",
+                   "variant": "FP64 ttrand_rounding + tt_rounding (reference algorithm, CPU restatement)",
+                   "sample": f"{sample} TT(s) of the batch per step"},
+        "cpu_baseline": {"value": v, "unit": "roundings/s", "cores": cores, "kind": "port",
+                         "sample": f"{sample} TT(s) per step (CPU restatement of the Julia path; Julia is absent)"},
+        "e2e": {"value": v, "unit": "roundings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------- ours
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=BATCH)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    import ttcuda
+
+    ctx = ttcuda.Context(local)
+    stream = torch.cuda.Stream(device=local)
+    ctx.set_stream(stream.cuda_stream)
+    ttcuda._CTX = ctx
+
+    dims, tts = workload(seed=7 + rank, batch=args.batch)
+    ranks = [r for _, r, _ in tts]
+    tt_objs = [ttcuda.TTvector(len(d_), v, d_, r, [0] * len(d_)) for d_, r, v in tts]
+    rks = heuristic(ranks)
+    block = max(rks)
+    s = ttcuda._sketch_ranks(dims, rks, block)
+    rho = ttcuda._rand_out_caps(dims, s)
+    xb = ttcuda.DeviceBatch.from_tts(tt_objs, ctx=ctx)
+    y_mixed = ttcuda.DeviceBatch(dims, [rho] * len(tts), ctx=ctx)
+    y_fp64 = ttcuda.DeviceBatch(dims, ranks, ctx=ctx)
+
+    def step_mixed(sync=False):
+        xb.round_rand(y_mixed, rks, orthogonal=False, seed=1234, block_rks=block, precision="bf16",
+                      after_tol=TOL, sync=sync)
+
+    def step_fp64(sync=False):
+        xb.round_det(y_fp64, tol=TOL, sync=sync)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def timed(fn, K):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            fn()
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # warm-up (builds and captures the plans)
+    for _ in range(max(3, args.warmup)):
+        step_mixed(sync=True)
+        step_fp64(sync=True)
+    ctx.synchronize()
+
+    # L2: the resident inputs (sum of core bytes) exceed the 126 MB L2
+    in_bytes = sum(8 * sum(d_[k] * r[k] * r[k + 1] for k in range(D)) for d_, r, _ in tts)
+
+    clock_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
+    os.makedirs(os.path.dirname(clock_path), exist_ok=True)
+    with ClockSampler(clock_path) as cs:
+        ms_mixed = timed(step_mixed, args.steps)
+        ms_fp64 = timed(step_fp64, args.steps)
+    ctx.synchronize()
+    clocks = cs.summary(local)
+
+    nb = len(tts) * world
+    value = nb * args.steps / (ms_mixed / 1e3)
+    fp64_value = nb * args.steps / (ms_fp64 / 1e3)
+
+    # accuracy on the GPU: ||x - round(x)|| / ||x|| through the library (difference TT, norm)
+    def rel_err(x, y):
+        d_ = ttcuda.tt_add(x, ttcuda.tt_scale(-1.0, ttcuda.TTvector(y.N, y.ttv_vec, y.ttv_dims, y.ttv_rks, [0] * y.N)))
+        return ttcuda.norm(d_) / ttcuda.norm(x)
+
+    out_m = y_mixed.download()
+    out_f = y_fp64.download()
+    nerr = min(4, len(tts))
+    err_mixed = max(rel_err(tt_objs[i], out_m[i]) for i in range(nerr))
+    err_fp64 = max(rel_err(tt_objs[i], out_f[i]) for i in range(nerr))
+    err_mf = max(rel_err(out_f[i], out_m[i]) for i in range(nerr))
+    ranks_equal = all(out_m[i].ttv_rks == out_f[i].ttv_rks for i in range(len(tts)))
+
+    # per-kernel profile of one extra step of each variant (event pair around every launch)
+    ctx.set_profiling(True)
+    step_mixed(sync=True)
+    prof_m = ctx.kernel_profile()
+    launches_m = ctx.stats()["kernel_launches"]
+    step_fp64(sync=True)
+    prof_f = ctx.kernel_profile()
+    launches_f = ctx.stats()["kernel_launches"]
+    ctx.set_profiling(False)
+
+    # FP64 peak of this GPU (cuBLAS DGEMM, best of 5): the roofline denominator of the FP64 kernels
+    a = torch.randn(4096, 4096, dtype=torch.float64, device=f"cuda:{local}")
+    bmat = torch.randn(4096, 4096, dtype=torch.float64, device=f"cuda:{local}")
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, bmat)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    fp64_peak_tflops = 2 * 4096 ** 3 / (best / 1e3) / 1e12
+    del a, bmat
+
+    # dominant kernel of the mixed step: device time per launch (event pair around each launch)
+    # and its algorithmic FLOPs per launch (the library's fixed conventions, from the launch shapes)
+    dom, (dom_ms, dom_n, dom_flops) = max(prof_m.items(), key=lambda kv: kv[1][0])
+    dom_avg_ms = dom_ms / max(1, dom_n)
+    achieved = (dom_flops / max(1, dom_n)) / (dom_avg_ms / 1e3) / 1e12 if dom_flops else None
+    flops_mixed = sum(v[2] for v in prof_m.values())
+    flops_fp64 = sum(v[2] for v in prof_f.values())
+
+    # end-to-end through the C ABI with host buffers (upload, round, download) every step
+    h2d = in_bytes
+    t0 = time.perf_counter()
+    d2h = 0
+    for _ in range(args.steps):
+        xb.upload(tt_objs)
+        step_mixed(sync=True)
+        outs = y_mixed.download()
+        d2h = sum(8 * sum(o_.ttv_dims[k] * o_.ttv_rks[k] * o_.ttv_rks[k + 1] for k in range(D)) for o_ in outs)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = nb * args.steps / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, secs = cpu_reference_rate(dims, tts, rks, 3)
+        cpu = {"value": rate, "unit": "roundings/s", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"first 3 TTs of the batch ({secs:.1f} s): FP64 ttrand_rounding + tt_rounding, "
+                         "numpy/LAPACK on all host threads"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "roundings/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 sketch + f64", "data": "synthetic",
+            "config": {"workload": f"batched rounding: {len(tts)} TTs per GPU, d=32, n=2, ranks U[16,256] (seeded), "
+                                   "sigma 10^(-i/32), tol 1e-8",
+                       "variant": "mixed: BF16-sketch (tcgen05) ttrand_rounding + FP64 SVD sweep",
+                       "sketch_ranks": "default_rank_heuristic (r + ceil(max r/2)), block_rks = max",
+                       "l2": f"inputs {in_bytes / 1e6:.0f} MB resident > 126 MB L2"},
+            "fp64": {"value": fp64_value, "unit": "roundings/s", "ms_per_step": ms_fp64 / args.steps,
+                     "variant": "deterministic tt_rounding (FP64 Householder QR sweep + Jacobi SVD sweep)"},
+            "mixed_over_fp64": value / fp64_value,
+            "accuracy": {"rel_err_mixed_max": err_mixed, "rel_err_fp64_max": err_fp64,
+                         "rel_diff_mixed_vs_fp64": err_mf, "ranks_identical": ranks_equal,
+                         "checked_tts": nerr},
+            "gflops_per_s": {"mixed_algorithmic": flops_mixed * world * args.steps
+                             / (ms_mixed / 1e3) / 1e9,
+                             "fp64_algorithmic": flops_fp64 * world * args.steps / (ms_fp64 / 1e3) / 1e9},
+            "roofline": {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": fp64_peak_tflops,
+                         "unit": "TFLOP/s", "frac": (achieved / fp64_peak_tflops) if achieved else None,
+                         "traffic": None,
+                         "peak_source": "FP64 cuBLAS DGEMM 4096^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+                         "avg_launch_ms": dom_avg_ms, "launches_per_step": dom_n,
+                         "profile_ms_per_step": {k: round(v[0], 3) for k, v in prof_m.items() if v[1]},
+                         "profile_gflop_per_step": {k: round(v[2] / 1e9, 3) for k, v in prof_m.items() if v[1]}},
+            "kernel_profile_fp64_ms": {k: round(v[0], 3) for k, v in prof_f.items() if v[1]},
+            "e2e": {"value": e2e_value, "unit": "roundings/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches_m * args.steps + launches_f * args.steps),
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -93,7 +93,20 @@ typedef struct {
   const double* const* sketch_blocks;
 } ttc_sketch_opts;
 
-/* Per-stage device times of the last call (CUDA events on the context stream), ms. */
+/* Kernel families reported by the per-kernel profile (ttc_set_profiling). */
+enum {
+  TTC_KERN_GEMM_F64 = 0,   /* grouped FP64 GEMM (contractions)              */
+  TTC_KERN_QR = 1,         /* batched Householder QR                        */
+  TTC_KERN_JACOBI = 2,     /* batched one-sided Jacobi SVD                  */
+  TTC_KERN_GEMM_BF16 = 3,  /* tcgen05 BF16 GEMM (sketch contractions)       */
+  TTC_KERN_APPLY = 4,      /* MPO x TT apply                                */
+  TTC_KERN_OTHER = 5,      /* copies, truncation rule, sketch generation... */
+  TTC_KERN_KINDS = 8
+};
+
+/* Per-stage device times of the last call (CUDA events on the context stream), ms.
+ * With profiling on, kind_ms / kind_launches hold per-kernel-family device times of the
+ * last call, measured with an event pair around every launch (no graph replay). */
 typedef struct {
   double total_ms;
   double sketch_ms;
@@ -102,7 +115,16 @@ typedef struct {
   double h2d_ms;
   double d2h_ms;
   int64_t kernel_launches;
+  double kind_ms[8];
+  int64_t kind_launches[8];
+  /* algorithmic FLOPs of each kernel family in the last profiled call (fixed conventions:
+     GEMM 2mnk; Householder QR 2mn^2-2n^3/3, doubled when Q is formed; one-sided Jacobi SVD
+     of an m x n block 4mn^2+8n^3) */
+  double kind_flops[8];
 } ttc_stats;
+
+/* Per-kernel-family timing of subsequent calls (0 = off, the default). */
+int ttc_set_profiling(ttc_context* ctx, int on);
 
 /* ---- context (no reference counterpart: the reference runs in one Julia process) ---- */
 int ttc_create(ttc_context** ctx, int device);

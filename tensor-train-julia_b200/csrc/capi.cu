@@ -326,6 +326,12 @@ int ttc_get_stats(const ttc_context* c, ttc_stats* out) {
   return TTC_OK;
 }
 
+int ttc_set_profiling(ttc_context* c, int on) {
+  if (!c) return TTC_EARG;
+  c->profiling = (on != 0);
+  return TTC_OK;
+}
+
 int ttc_synchronize(ttc_context* c) {
   if (!c) return TTC_EARG;
   return guard(c, [&] {

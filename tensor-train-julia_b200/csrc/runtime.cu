@@ -66,9 +66,15 @@ Plan::~Plan() {
   if (d_blob) { region_remove(d_blob); cudaFree(d_blob); }
 }
 
+static void launch_op(ttc_context* c, const Plan& p, const Op& op);
+
 static void launch_ops(ttc_context* c, Plan& p) {
+  for (const Op& op : p.ops) launch_op(c, p, op);
+}
+
+static void launch_op(ttc_context* c, const Plan& p, const Op& op) {
   cudaStream_t s = c->stream;
-  for (const Op& op : p.ops) {
+  {
     const unsigned char* d = p.d_blob + op.off;
     switch (op.kind) {
       case OP_GEMM: launch_gemm_f64((const GemmDesc*)d, op.count, op.total, s); break;
@@ -97,8 +103,61 @@ long long count_launches(const Plan& p) {
   return n;
 }
 
+static int op_kind(OpKind k) {
+  switch (k) {
+    case OP_GEMM: return TTC_KERN_GEMM_F64;
+    case OP_QR: return TTC_KERN_QR;
+    case OP_JACOBI: return TTC_KERN_JACOBI;
+    case OP_BF16GEMM: return TTC_KERN_GEMM_BF16;
+    case OP_APPLY: return TTC_KERN_APPLY;
+    default: return TTC_KERN_OTHER;
+  }
+}
+
+// Profiled execution: an event pair around every launch, times accumulated per kernel family.
+static void run_plan_profiled(ttc_context* c, Plan& p) {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> kinds;
+  std::vector<double> flops;
+  for (const Op& op : p.ops) {
+    if (op.kind == OP_STAGE) continue;
+    flops.push_back(op.flops);
+    cudaEvent_t a, b;
+    TTC_CUDA(cudaEventCreate(&a));
+    TTC_CUDA(cudaEventCreate(&b));
+    ev.push_back(a);
+    ev.push_back(b);
+    kinds.push_back(op_kind(op.kind));
+  }
+  size_t i = 0;
+  for (const Op& op : p.ops) {
+    if (op.kind == OP_STAGE) {
+      TTC_CUDA(cudaEventRecord(c->ev[op.a], c->stream));
+      continue;
+    }
+    TTC_CUDA(cudaEventRecord(ev[2 * i], c->stream));
+    launch_op(c, p, op);
+    TTC_CUDA(cudaEventRecord(ev[2 * i + 1], c->stream));
+    ++i;
+  }
+  TTC_CUDA(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 8; ++k) { c->stats.kind_ms[k] = 0; c->stats.kind_launches[k] = 0; c->stats.kind_flops[k] = 0; }
+  for (size_t j = 0; j < kinds.size(); ++j) {
+    float ms = 0;
+    TTC_CUDA(cudaEventElapsedTime(&ms, ev[2 * j], ev[2 * j + 1]));
+    c->stats.kind_ms[kinds[j]] += ms;
+    c->stats.kind_launches[kinds[j]] += 1;
+    c->stats.kind_flops[kinds[j]] += flops[j];
+  }
+  for (auto e : ev) cudaEventDestroy(e);
+}
+
 void run_plan(ttc_context* c, Plan& p) {
   c->stats.kernel_launches = count_launches(p);
+  if (c->profiling) {
+    run_plan_profiled(c, p);
+    return;
+  }
   if (p.gexec && p.graph_stream == c->stream) {
     TTC_CUDA(cudaGraphLaunch(p.gexec, c->stream));
     return;
@@ -189,6 +248,7 @@ void Builder::gemm(std::vector<GemmDesc> v) {
   }
   if (w.empty()) return;
   Op op; op.kind = OP_GEMM; op.off = plan->push(w); op.count = (int)w.size(); op.total = t;
+  for (auto& d : w) op.flops += 2.0 * d.m * d.n * d.k * std::max(1, d.batch);
   plan->ops.push_back(op);
 }
 void Builder::qr(const std::vector<QRDesc>& v) {
@@ -206,6 +266,10 @@ void Builder::qr(const std::vector<QRDesc>& v) {
     TTC_REQUIRE(d.lda >= d.m && (!d.Q || d.ldq >= d.m) && (!d.R || d.ldr >= K), TTC_EINTERNAL, "qr: leading dims");
   }
   Op op; op.kind = OP_QR; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm;
+  for (auto& d : v) {
+    const double m = d.m, k = std::min(d.m, d.n);
+    op.flops += (d.Q ? 2.0 : 1.0) * (2.0 * m * k * k - 2.0 * k * k * k / 3.0) + 2.0 * m * k * (d.n - k);
+  }
   plan->ops.push_back(op);
 }
 void Builder::jacobi(const std::vector<JacobiDesc>& v) {
@@ -223,6 +287,7 @@ void Builder::jacobi(const std::vector<JacobiDesc>& v) {
     TTC_REQUIRE(2LL * 1 * (d.m + (d.W ? d.n : 0)) <= 25600 && d.n <= 25600, TTC_EDIM, "jacobi: matrix too large");
   }
   Op op; op.kind = OP_JACOBI; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm; op.b = nn;
+  for (auto& d : v) op.flops += 4.0 * d.m * (double)d.n * d.n + 8.0 * (double)d.n * d.n * d.n;
   plan->ops.push_back(op);
 }
 void Builder::trunc(const std::vector<TruncDesc>& v, double tol, long long rmax) {
@@ -336,6 +401,7 @@ void Builder::bf16gemm(std::vector<Bf16GemmDesc> v) {
   }
   if (w.empty()) return;
   Op op; op.kind = OP_BF16GEMM; op.off = plan->push(w); op.count = (int)w.size(); op.total = t;
+  for (auto& d : w) op.flops += 2.0 * d.m * d.n * d.k;
   plan->ops.push_back(op);
 }
 void Builder::cvt_bf16(const std::vector<CvtDesc>& v) {

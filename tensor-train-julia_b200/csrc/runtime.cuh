@@ -31,6 +31,7 @@ struct Op {
   int a = 0, b = 0;    // kernel-specific (max_m, max_n, stage id ...)
   double tol = 0.0;
   long long rmax = 0;
+  double flops = 0.0;  // algorithmic FLOPs of the launch (profiling only)
 };
 
 // "Finalize" descriptor: if *flag != 0, zero the TT's cores and restore its ranks.
@@ -91,6 +92,7 @@ struct ttc_context {
   size_t stage_bytes = 0;
   double* d_sk = nullptr;           // host-provided sketch blocks
   size_t sk_cap = 0;
+  bool profiling = false;           // per-kernel-family event timing (ttc_set_profiling)
 };
 
 struct ttc_batch {

@@ -6,6 +6,17 @@
 // GEMM 1 writes T directly as the K-major BF16 operand of GEMM 2; GEMM 2 writes W_k in
 // FP64 (for the FP64 range finder Z = y_k W_{k+1}) and as the K-major BF16 operand of the
 // next site's GEMM 1.  Cores and sketch blocks are converted to BF16 once per call.
+//
+// Precision policy.  The range finder Z = y_{k-1} W_k recovers the TT exactly (s_k >= r_k)
+// when range(y_{k-1} W_k) contains range(y_{k-1} R_k), R_k the right interface of bond k.
+// That holds for ANY perturbed W_k of full row rank when R_k has full row rank, so BF16
+// rounding is harmless there.  When R_k is rank deficient (a non-minimal TT: r_k larger
+// than n_k times the rank of R_{k+1}, e.g. sums of TTs or independently drawn ranks), W_k
+// must stay of the form R_k X, which rounding A_k or W_{k+1} to BF16 breaks (the captured
+// subspace then moves by ~1e-3).  Levels whose right interface is structurally rank
+// deficient, rho_k = min(r_k, n_k rho_{k+1}) < r_k, are therefore contracted in FP64 from
+// the FP64 W_{k+1}; their BF16 copy of W_k is made afterwards for the next BF16 level.
+// Numerically (not structurally) deficient interfaces are not detected.
 #include <algorithm>
 
 #include "drivers.cuh"
@@ -30,11 +41,23 @@ void emit_sketch_bf16(Builder& B, ttc_batch* x, const std::vector<int>& tts, con
   std::vector<std::vector<void*>> A16(T, std::vector<void*>(N)), W16(T, std::vector<void*>(N + 1));
   std::vector<void*> S16(N);
   std::vector<CvtDesc> cv;
+  // f64lvl[i][k]: the right interface of bond k of TT i is structurally rank deficient
+  std::vector<std::vector<char>> f64lvl(T, std::vector<char>(N + 1, 0));
+  for (size_t i = 0; i < T; ++i) {
+    long long rho = 1;
+    for (int k = N - 1; k >= 0; --k) {
+      rho = std::min<long long>(x->rk(tts[i], k), x->dims[k] * rho);
+      f64lvl[i][k] = rho < x->rk(tts[i], k);
+    }
+  }
   for (size_t i = 0; i < T; ++i) {
     const int t = tts[i];
     for (int k = 0; k < N; ++k) {
       const long long n = x->dims[k], r0 = x->rk(t, k), r1 = x->rk(t, k + 1), xc = x->capr(t, k);
       const long long lda = pad8(r1);
+      W[i][k] = B.wd((size_t)r0 * sp.b[k] * sp.p[k]);
+      W16[i][k] = (k > 0) ? bf(pad8(r0) * sp.b[k] * sp.p[k]) : nullptr;
+      if (f64lvl[i][k]) continue;
       A16[i][k] = bf(r0 * n * lda);
       for (long long z = 0; z < n; ++z) {
         CvtDesc c{};
@@ -46,8 +69,6 @@ void emit_sketch_bf16(Builder& B, ttc_batch* x, const std::vector<int>& tts, con
         c.alpha = 1.0;
         cv.push_back(c);
       }
-      W[i][k] = B.wd((size_t)r0 * sp.b[k] * sp.p[k]);
-      W16[i][k] = (k > 0) ? bf(pad8(r0) * sp.b[k] * sp.p[k]) : nullptr;
     }
     W[i][N] = B.ctx->d_one;
     W16[i][N] = bf(8);
@@ -77,12 +98,43 @@ void emit_sketch_bf16(Builder& B, ttc_batch* x, const std::vector<int>& tts, con
     const size_t mk = B.mark();
     std::vector<ZeroDesc> zt;
     std::vector<Bf16GemmDesc> g1, g2;
+    std::vector<GemmDesc> f1, f2;
+    std::vector<CvtDesc> cw;
     const long long n = x->dims[k], bl = sp.b[k + 1], br = sp.b[k], pk = sp.p[k];
     const long long ldt = pad8(n * bl), lds = pad8(n * bl);
     for (size_t i = 0; i < T; ++i) {
       const int t = tts[i];
       const long long r0 = x->rk(t, k), r1 = x->rk(t, k + 1);
       const long long ldw1 = pad8(r1), ldw0 = pad8(r0);
+      if (f64lvl[i][k]) {
+        // FP64 level: T[(a,z), be] = sum_al A_k[a,z,al] W_{k+1}[al,be,j]; W_k = T S_k
+        const long long xc = x->capr(t, k);
+        double* Tm = B.wd((size_t)(r0 * n * bl * pk));
+        GemmDesc d = gd((int)(r0 * n), (int)bl, (int)r1, x->core(t, k), 1, xc * n, W[i][k + 1], 1, r1, Tm, 1, r0 * n);
+        d.m0 = (int)r0; d.a_i0 = 1; d.a_i1 = xc;
+        d.c_i0 = 1; d.c_i1 = r0;
+        d.batch = (int)pk;
+        d.a_b = 0;
+        d.b_b = (k < N - 1) ? r1 * bl : 0;
+        d.c_b = r0 * n * bl;
+        f1.push_back(d);
+        GemmDesc e = gd((int)r0, (int)br, (int)(n * bl), Tm, 1, r0, S[k], 1, n * bl, W[i][k], 1, r0);
+        e.batch = (int)pk;
+        e.a_b = r0 * n * bl;
+        e.b_b = n * bl * br;
+        e.c_b = r0 * br;
+        f2.push_back(e);
+        if (k > 0) {   // BF16 copy of W_k (a, (b, j)) at a + ldw0 (b + br j)
+          CvtDesc c{};
+          c.src = W[i][k]; c.dst = W16[i][k];
+          c.rows = r0; c.cols = br * pk;
+          c.ss_i = 1; c.ss_j = r0;
+          c.ds_i = 1; c.ds_j = ldw0;
+          c.alpha = 1.0;
+          cw.push_back(c);
+        }
+        continue;
+      }
       const long long tnd = (r0 * ldt * pk + 3) / 4;
       double* Tbuf = B.wd((size_t)tnd);
       zt.push_back({Tbuf, tnd});
@@ -109,6 +161,9 @@ void emit_sketch_bf16(Builder& B, ttc_batch* x, const std::vector<int>& tts, con
     B.zero(zt);
     B.bf16gemm(g1);
     B.bf16gemm(g2);
+    B.gemm(f1);
+    B.gemm(f2);
+    B.cvt_bf16(cw);
     B.release(mk);
   }
 }

@@ -150,6 +150,20 @@ class Context:
     def synchronize(self):
         self.check(lib.ttc_synchronize(self.h))
 
+    def set_stream(self, cuda_stream_handle: int):
+        """Run subsequent calls on an existing CUDA stream (e.g. torch's cuda_stream handle)."""
+        self.check(lib.ttc_set_stream(self.h, C.c_void_p(cuda_stream_handle)))
+
+    def set_profiling(self, on: bool):
+        self.check(lib.ttc_set_profiling(self.h, 1 if on else 0))
+
+    def kernel_profile(self) -> dict:
+        """Per-kernel-family (device ms, launches, algorithmic FLOPs) of the last call (profiling on)."""
+        s = L.Stats()
+        self.check(lib.ttc_get_stats(self.h, C.byref(s)))
+        return {name: (s.kind_ms[i], int(s.kind_launches[i]), s.kind_flops[i])
+                for i, name in enumerate(L.KERNEL_KINDS)}
+
     def close(self):
         if self.h:
             lib.ttc_destroy(self.h)

@@ -39,7 +39,11 @@ class SketchOpts(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("total_ms", f64), ("sketch_ms", f64), ("orth_ms", f64), ("svd_ms", f64), ("h2d_ms", f64),
-                ("d2h_ms", f64), ("kernel_launches", i64)]
+                ("d2h_ms", f64), ("kernel_launches", i64), ("kind_ms", f64 * 8), ("kind_launches", i64 * 8),
+                ("kind_flops", f64 * 8)]
+
+
+KERNEL_KINDS = ["gemm_f64", "householder_qr", "jacobi_svd", "gemm_bf16_tcgen05", "mpo_apply", "other"]
 
 
 def _load():
@@ -57,6 +61,7 @@ _SIGS = {
     "ttc_set_stream": (i32, [vp, vp]),
     "ttc_last_error": (C.c_char_p, [vp]),
     "ttc_get_stats": (i32, [vp, C.POINTER(Stats)]),
+    "ttc_set_profiling": (i32, [vp, C.c_int]),
     "ttc_synchronize": (i32, [vp]),
     "ttc_batch_create": (i32, [vp, i32, i32, P_i64, P_i64, C.POINTER(vp)]),
     "ttc_batch_destroy": (i32, [vp]),

@@ -79,4 +79,5 @@ def decaying_tt(dims, ranks, seed, decay_per=32.0):
         core = core * prev[None, :, None]
         vec.append(np.asfortranarray(core))
         prev = 10.0 ** (-np.arange(b) / decay_per)
+        prev /= np.sqrt(np.mean(prev ** 2))      # unit RMS: the TT norm stays O(1) along the train
     return o.TTvector(N, vec, tuple(dims), list(ranks), [0] * N)

@@ -337,3 +337,47 @@ def test_batched_round_rand_then_svd():
             ref = o.tt_rounding(o.ttrand_rounding(t, rks, orthogonal=False, seed=4, block_rks=64), tol=1e-5)
             assert got.ttv_rks == ref.ttv_rks
             assert rel(got, ref) < (1e-10 if prec == "fp64" else 1e-7)
+
+
+# ------------------------------------------------------ mixed precision on non-minimal TTs
+@pytest.mark.parametrize("block", [None, 8, 16, 64])
+@pytest.mark.parametrize("orthogonal", [False, True])
+def test_ttrand_bf16_sum_of_tts_exact(block, orthogonal):
+    """Sum of three rank-4 TTs (ranks not re-clamped, so the right interfaces of the last
+    bonds are rank deficient): the BF16 sketch still reconstructs the TT to FP64 accuracy,
+    because rank-deficient levels are contracted in FP64."""
+    g = np.random.default_rng(5)
+    dims = (2,) * 10
+    x = None
+    for _ in range(3):
+        t = o.rand_tt(dims, [1] + [4] * 9 + [1], g)
+        x = t if x is None else o.tt_add(x, t)
+    rks = [1] + [16] * 9 + [1]
+    got = ttcuda.ttrand_rounding(to_dev(x), rks, orthogonal=orthogonal, seed=11, precision="bf16", block_rks=block)
+    ref = o.ttrand_rounding(x, rks, orthogonal=orthogonal, seed=11, block_rks=block)
+    assert got.ttv_rks == ref.ttv_rks
+    assert rel(got, x) < 1e-11
+
+
+def test_batched_round_rand_bf16_iid_ranks():
+    """Independently drawn interior ranks (bonds wider than n times a neighbour), decaying
+    spectrum: mixed-precision randomized rounding plus the FP64 SVD sweep meets the FP64
+    deterministic rounding at tol 1e-8 with identical truncation ranks."""
+    g = np.random.default_rng(31)
+    dims = (2,) * 16
+    tts = []
+    for i in range(4):
+        r = [1] + [int(v) for v in g.integers(4, 48, size=15)] + [1]
+        tts.append(decaying_tt(dims, o.r_and_d_to_rks(r, dims, rmax=max(r)), seed=300 + i, decay_per=4.0))
+    rks = o.default_rank_heuristic(tts)
+    xb = ttcuda.DeviceBatch.from_tts([to_dev(t) for t in tts])
+    block = max(rks)
+    s = ttcuda._sketch_ranks(dims, rks, block)
+    yb = ttcuda.DeviceBatch(dims, [ttcuda._rand_out_caps(dims, s)] * len(tts))
+    xb.round_rand(yb, rks, orthogonal=False, seed=9, block_rks=block, precision="bf16", after_tol=1e-8)
+    for t, got in zip(tts, yb.download()):
+        ref = o.tt_rounding(t, tol=1e-8)
+        assert got.ttv_rks == ref.ttv_rks
+        assert rel(got, ref) < 1e-8
+        # floor() keeps the discarded weight of each bond below tol^2 ||x||^2 (src/tt_rounding.jl:298-315)
+        assert rel(got, t) < math.sqrt(len(dims) - 1) * 1e-8
