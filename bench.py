@@ -292,12 +292,20 @@ def main():
 
     # per-kernel profile of one extra step of each variant (event pair around every launch)
     ctx.set_profiling(True)
+
+    def sweeps(st):
+        n_ = max(1, st["jacobi_problems"])
+        return {"problems": st["jacobi_problems"], "mean": round(st["jacobi_sweeps_sum"] / n_, 2),
+                "max": st["jacobi_sweeps_max"]}
+
     step_mixed(sync=True)
     prof_m = ctx.kernel_profile()
-    launches_m = ctx.stats()["kernel_launches"]
+    st = ctx.stats()
+    launches_m, sw_m = st["kernel_launches"], sweeps(st)
     step_fp64(sync=True)
     prof_f = ctx.kernel_profile()
-    launches_f = ctx.stats()["kernel_launches"]
+    st = ctx.stats()
+    launches_f, sw_f = st["kernel_launches"], sweeps(st)
     ctx.set_profiling(False)
 
     # FP64 peak of this GPU (cuBLAS DGEMM, best of 5): the roofline denominator of the FP64 kernels
@@ -373,6 +381,7 @@ def main():
                          "profile_ms_per_step": {k: round(v[0], 3) for k, v in prof_m.items() if v[1]},
                          "profile_gflop_per_step": {k: round(v[2] / 1e9, 3) for k, v in prof_m.items() if v[1]}},
             "kernel_profile_fp64_ms": {k: round(v[0], 3) for k, v in prof_f.items() if v[1]},
+            "jacobi_sweeps": {"mixed": sw_m, "fp64": sw_f},
             "e2e": {"value": e2e_value, "unit": "roundings/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches_m * args.steps + launches_f * args.steps),

@@ -121,6 +121,8 @@ typedef struct {
      GEMM 2mnk; Householder QR 2mn^2-2n^3/3, doubled when Q is formed; one-sided Jacobi SVD
      of an m x n block 4mn^2+8n^3) */
   double kind_flops[8];
+  /* one-sided Jacobi SVDs of the last profiled call: problems, total and largest sweep count */
+  int64_t jacobi_problems, jacobi_sweeps_sum, jacobi_sweeps_max;
 } ttc_stats;
 
 /* Per-kernel-family timing of subsequent calls (0 = off, the default). */

@@ -22,6 +22,9 @@ struct Builder {
   void release(size_t m) { wsoff = m; }
   void stage(int id);
   const int* const_ints(const std::vector<int>& v);
+  // n ints in the plan's device blob that kernels may write (diagnostics such as Jacobi
+  // sweep counts); read back by the profiled run.
+  int* diag_ints(int n);
 
   void gemm(std::vector<GemmDesc> v);
   void qr(const std::vector<QRDesc>& v);

@@ -34,7 +34,7 @@ struct JacobiDesc {
   int* perm;        // n
   int* info;        // optional: sweeps used (negative if the sweep cap was hit)
 };
-void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, cudaStream_t s,
+void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, bool accw, cudaStream_t s,
                    int* d_flags);
 
 // ---- truncation rule (tt_kernels.cu): floor(s, tol) then min(k, rmax, #(s>0))

@@ -12,7 +12,20 @@
 // I - V T V^T (dlarft) is applied to the trailing columns by warps that own two
 // columns each (V is read from shared memory once per pair of columns), and Q is formed
 // backwards from the stored panels (dorgqr).
+//
+// One thread-block cluster of C CTAs per problem.  Every CTA factors each panel itself
+// (same data, same arithmetic: identical reflectors, no broadcast needed); the column pairs
+// (2p, 2p+1) of the trailing update and of Q are owned by CTA p mod C, so a column is always
+// updated by the same CTA.  A cluster barrier (release/acquire at cluster scope) after each
+// panel's trailing update makes the next panel visible to every CTA.  CTA 0 writes the
+// factored panels and the T factors, which the Q formation reads after one more barrier.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
 #include "kernels.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace ttc {
 namespace {
@@ -39,20 +52,49 @@ __device__ double block_sum(double v, double* red) {
   return s;
 }
 
+// Copy `cols` columns of `rows` doubles (one warp per column, lanes over rows, four loads in
+// flight per lane); returns whether a non-finite value was copied.
+__device__ __forceinline__ bool copy_cols(double* __restrict__ dst, long long dld, const double* __restrict__ src,
+                                          long long sld, int rows, int cols) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  bool bad = false;
+  for (int c = warp; c < cols; c += NW) {
+    const double* sc = src + (long long)c * sld;
+    double* dc = dst + (long long)c * dld;
+    for (int r0 = lane; r0 < rows; r0 += 128) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = (r0 + 32 * u < rows) ? sc[r0 + 32 * u] : 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (r0 + 32 * u < rows) { dc[r0 + 32 * u] = v[u]; bad |= !isfinite(v[u]); }
+    }
+  }
+  return bad;
+}
+
 // Apply (I - V T^T V^T) [trans=1] or (I - V T V^T) [trans=0] to columns [c_begin, c_end) of
 // the global matrix M (rows r0..m-1, ld), with V (mp x jb) in shared memory (column-major,
 // stride mp_ld, unit diagonal implied, zeros above) and T (jb x jb) in shared memory.
+// Column pairs (2p, 2p+1) with p mod csize == crank belong to this CTA.
 __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_begin, int c_end,
-                                      const double* V, int mp_ld, int jb, const double* T, bool trans) {
+                                      const double* V, int mp_ld, int jb, const double* T, bool trans,
+                                      int crank, int csize) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int mp = m - r0;
-  for (int c = c_begin + 2 * warp; c < c_end; c += 2 * NW) {
-    const bool two = (c + 1 < c_end);
-    double* col0 = M + (long long)c * ld + r0;
+  const int p_begin = c_begin >> 1, p_end = (c_end + 1) >> 1;
+  const int p_first = p_begin + ((crank - p_begin) % csize + csize) % csize;
+  for (int p = p_first + warp * csize; p < p_end; p += NW * csize) {
+    const int c = 2 * p;
+    if (c + 1 < c_begin) continue;
+    // a pair may straddle c_begin (odd start) or c_end: update only the columns inside
+    const bool has0 = (c >= c_begin), two = has0 ? (c + 1 < c_end) : false;
+    double* col0 = M + (long long)(has0 ? c : c + 1) * ld + r0;
     double* col1 = M + (long long)(c + 1) * ld + r0;
     double w0[NB], w1[NB];
 #pragma unroll
     for (int l = 0; l < NB; ++l) { w0[l] = 0.0; w1[l] = 0.0; }
+#pragma unroll 4
     for (int r = lane; r < mp; r += 32) {
       const double x0 = col0[r];
       const double x1 = two ? col1[r] : 0.0;
@@ -69,32 +111,41 @@ __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_be
     for (int l = 0; l < NB; ++l) {
       if (l < jb) { w0[l] = warp_sum(w0[l]); w1[l] = warp_sum(w1[l]); }
     }
-    // u = T^T w (trans) or T w, T upper triangular.
-    double u0[NB], u1[NB];
+    // u = T^T w (trans) or T w, T upper triangular, computed in place: u_l = sum_{i<=l}
+    // T[i,l] w_i needs only w_0..w_l (descending l); u_l = sum_{i>=l} T[l,i] w_i needs only
+    // w_l..w_{jb-1} (ascending l).
+    if (trans) {
 #pragma unroll
-    for (int l = 0; l < NB; ++l) {
-      double a0 = 0.0, a1 = 0.0;
-      if (l < jb) {
-        if (trans) {
+      for (int l = NB - 1; l >= 0; --l) {
+        double a0 = 0.0, a1 = 0.0;
+        if (l < jb) {
 #pragma unroll
           for (int i = 0; i < NB; ++i)
             if (i <= l) { a0 = fma(T[l * NB + i], w0[i], a0); a1 = fma(T[l * NB + i], w1[i], a1); }
-        } else {
+        }
+        w0[l] = a0; w1[l] = a1;
+      }
+    } else {
+#pragma unroll
+      for (int l = 0; l < NB; ++l) {
+        double a0 = 0.0, a1 = 0.0;
+        if (l < jb) {
 #pragma unroll
           for (int i = 0; i < NB; ++i)
             if (i >= l && i < jb) { a0 = fma(T[i * NB + l], w0[i], a0); a1 = fma(T[i * NB + l], w1[i], a1); }
         }
+        w0[l] = a0; w1[l] = a1;
       }
-      u0[l] = a0; u1[l] = a1;
     }
+#pragma unroll 4
     for (int r = lane; r < mp; r += 32) {
       double d0 = 0.0, d1 = 0.0;
 #pragma unroll
       for (int l = 0; l < NB; ++l) {
         if (l < jb) {
           const double v = (r > l) ? V[l * mp_ld + r] : (r == l ? 1.0 : 0.0);
-          d0 = fma(v, u0[l], d0);
-          d1 = fma(v, u1[l], d1);
+          d0 = fma(v, w0[l], d0);
+          d1 = fma(v, w1[l], d1);
         }
       }
       col0[r] -= d0;
@@ -105,9 +156,11 @@ __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_be
 }  // namespace
 
 // T layout in shared memory: T[col * NB + row] (upper triangular).
-__global__ void __launch_bounds__(NT) householder_qr_kernel(const QRDesc* __restrict__ descs, int* flags) {
+__global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __restrict__ descs, int csize, int* flags) {
   extern __shared__ double sm[];
-  const QRDesc D = descs[blockIdx.x];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int crank = (int)cluster.block_rank();
+  const QRDesc D = descs[blockIdx.x / csize];
   const int m = D.m, n = D.n;
   if (m <= 0 || n <= 0) return;
   const int K = min(m, n);
@@ -126,12 +179,7 @@ __global__ void __launch_bounds__(NT) householder_qr_kernel(const QRDesc* __rest
     const int mp = m - j0;
     const int mp_ld = mp;
     // 1. load panel
-    for (int e = tid; e < mp * jb; e += NT) {
-      const int c = e / mp, r = e - c * mp;
-      const double v = A[(long long)(j0 + c) * lda + j0 + r];
-      nonfinite |= !isfinite(v);
-      P[c * mp_ld + r] = v;
-    }
+    nonfinite |= copy_cols(P, mp_ld, A + (long long)j0 * lda + j0, lda, mp, jb);
     __syncthreads();
     // 2. factor panel
     for (int jj = 0; jj < jb; ++jj) {
@@ -195,43 +243,39 @@ __global__ void __launch_bounds__(NT) householder_qr_kernel(const QRDesc* __rest
       }
     }
     __syncthreads();
-    // 4. trailing update with H^T = I - V T^T V^T
-    if (j0 + jb < n) apply_block_reflector(A, lda, j0, m, j0 + jb, n, P, mp_ld, jb, T, true);
-    // 5. write back the panel and keep T
-    for (int e = tid; e < mp * jb; e += NT) {
-      const int c = e / mp, r = e - c * mp;
-      A[(long long)(j0 + c) * lda + j0 + r] = P[c * mp_ld + r];
+    // 4. trailing update with H^T = I - V T^T V^T (this CTA's column pairs)
+    if (j0 + jb < n) apply_block_reflector(A, lda, j0, m, j0 + jb, n, P, mp_ld, jb, T, true, crank, csize);
+    // 5. CTA 0 writes back the panel and keeps T
+    if (crank == 0) {
+      copy_cols(A + (long long)j0 * lda + j0, lda, P, mp_ld, mp, jb);
+      if (D.Tws)
+        for (int e = tid; e < NB * NB; e += NT) D.Tws[(j0 / NB) * NB * NB + e] = T[e];
     }
-    if (D.Tws)
-      for (int e = tid; e < NB * NB; e += NT) D.Tws[(j0 / NB) * NB * NB + e] = T[e];
-    __syncthreads();
+    cluster.sync();   // trailing columns and the panel visible to every CTA
   }
-  if (nonfinite) atomicOr(flags, DFLAG_NONFINITE);
+  if (nonfinite && crank == 0 && threadIdx.x == 0) atomicOr(flags, DFLAG_NONFINITE);
 
   // R = upper triangle of A[0:K, 0:n]
   if (D.R) {
-    for (long long e = tid; e < (long long)K * n; e += NT) {
-      const int j = (int)(e / K), i = (int)(e - (long long)j * K);
-      D.R[(long long)j * D.ldr + i] = (i <= j) ? A[(long long)j * lda + i] : 0.0;
-    }
+    for (int j = (int)(threadIdx.x >> 5) + NW * crank; j < n; j += NW * csize)
+      for (int i = (int)(threadIdx.x & 31); i < K; i += 32)
+        D.R[(long long)j * D.ldr + i] = (i <= j) ? A[(long long)j * lda + i] : 0.0;
   }
   if (!D.Q) return;
-  // Q = H_1 ... H_K [I; 0], accumulated backwards panel by panel.
-  for (long long e = tid; e < (long long)m * K; e += NT) {
-    const int j = (int)(e / m), i = (int)(e - (long long)j * m);
-    D.Q[(long long)j * D.ldq + i] = (i == j) ? 1.0 : 0.0;
+  // Q = H_1 ... H_K [I; 0], accumulated backwards panel by panel.  Each CTA initialises
+  // and updates only its own column pairs, so the panels need no barrier between them.
+  for (int c = 0; c < K; ++c) {
+    if (((c >> 1) % csize) != crank) continue;
+    for (int i = tid; i < m; i += NT) D.Q[(long long)c * D.ldq + i] = (i == c) ? 1.0 : 0.0;
   }
   __syncthreads();
   const int npan = (K + NB - 1) / NB;
   for (int p = npan - 1; p >= 0; --p) {
     const int j0 = p * NB, jb = min(NB, K - j0), mp = m - j0, mp_ld = mp;
-    for (int e = tid; e < mp * jb; e += NT) {
-      const int c = e / mp, r = e - c * mp;
-      P[c * mp_ld + r] = A[(long long)(j0 + c) * lda + j0 + r];
-    }
+    copy_cols(P, mp_ld, A + (long long)j0 * lda + j0, lda, mp, jb);
     for (int e = tid; e < NB * NB; e += NT) T[e] = D.Tws[p * NB * NB + e];
     __syncthreads();
-    apply_block_reflector(D.Q, D.ldq, j0, m, j0, K, P, mp_ld, jb, T, false);
+    apply_block_reflector(D.Q, D.ldq, j0, m, j0, K, P, mp_ld, jb, T, false, crank, csize);
     __syncthreads();
   }
 }
@@ -240,13 +284,36 @@ void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int*
   if (count <= 0) return;
   TTC_REQUIRE(max_m <= QR_MAX_M, TTC_EDIM, "qr: row count exceeds the supported maximum (1536)");
   const size_t smem = sizeof(double) * (NB * NB * 2 + NB + NW + (size_t)max_m * NB);
-  static bool attr_set = false;
-  if (!attr_set) {
+  static int attr_dev = -1;
+  static int nsm = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
     TTC_CUDA(cudaFuncSetAttribute(householder_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(double) * (NB * NB * 2 + NB + NW + (size_t)QR_MAX_M * NB))));
-    attr_set = true;
+    TTC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    attr_dev = dev;
   }
-  householder_qr_kernel<<<count, NT, smem, s>>>(d_descs, d_flags);
+  // CTAs per problem: fill the resident-CTA slots of the GPU, at most 8 (portable cluster)
+  int per_sm = 1;
+  TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, householder_qr_kernel, NT, smem));
+  const int slots = nsm * std::max(1, per_sm);
+  int c = std::min(8, std::max(1, slots / count));
+  int csize = 1;
+  while (csize * 2 <= c) csize *= 2;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)(count * csize));
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)csize;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  TTC_CUDA(cudaLaunchKernelEx(&cfg, householder_qr_kernel, d_descs, csize, d_flags));
   TTC_CHECK_LAUNCH();
 }
 

@@ -111,6 +111,7 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
     std::vector<TruncDesc> tr;
     std::vector<SelectDesc> sel;
     std::vector<GemmDesc> g1, g2, g3;
+    int* infos = B.diag_ints((int)T);
     const int n = (int)y->dims[j], nl = (int)y->dims[j - 1];
     for (size_t i = 0; i < T; ++i) {
       const int t = tts[i];
@@ -118,6 +119,7 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
       const int yc = y->capr(t, j), ycl = y->capr(t, j - 1);
       const int ml = ycl * nl;
       int* rank = y->drk(t, j);
+      int* info = infos + i;
       double* X = B.wd((size_t)p * q);
       double* T1 = B.wd((size_t)q * q);
       double* T2 = B.wd((size_t)ml * q);
@@ -140,30 +142,29 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         cpY.push_back(cd2(R, Y, q, q, 1, q, q, 1));
         qr2.push_back({q, q, Y, q, nullptr, 0, R2, q, Tws2});
         cpR.push_back(cd2(R2, Rc, q, q, 1, q, q, 1));
-        jac.push_back({q, q, Rc, q, nullptr, 0, sig, perm});
+        jac.push_back({q, q, Rc, q, nullptr, 0, sig, perm, info});
         tr.push_back({sig, perm, q, rank});
         sel.push_back({Rc, q, sig, perm, rank, q, q, q, Ut, q, 1});
         g1.push_back(gd(p, q, q, Q, 1, p, Ut, 1, q, y->core(t, j), yc, 1));
         g2.push_back(gd(q, q, q, R, q, 1, Ut, 1, q, T1, 1, q));
       } else {
-        double* Q = B.wd((size_t)q * p);
+        // M = Q1 R1 (q > p, Q1 not formed); one-sided Jacobi on R1^T (p x p) gives V Sigma
+        // in its columns: core j <- V^T (normalised columns, exactly orthonormal up to the
+        // rotation threshold), and the factor absorbed into core j-1 is M V = U Sigma.
         double* R = B.wd((size_t)p * p);
         double* Rc = B.wd((size_t)p * p);
-        double* W = B.wd((size_t)p * p);
         double* sig = B.wd(p);
         int* perm = B.wi(p);
         double* Tws = B.wd(qr_tws(q, p));
-        double* Wt = B.wd((size_t)p * q);
-        double* Bt = B.wd((size_t)p * q);
+        double* Vt = B.wd((size_t)p * q);
         cpX.push_back(cd2(y->core(t, j), X, q, p, 1, yc, 1, q));
-        qr.push_back({q, p, X, q, Q, q, R, p, Tws});
-        cpR.push_back(cd2(R, Rc, p, p, 1, p, 1, p));
-        jac.push_back({p, p, Rc, p, W, p, sig, perm});
+        qr.push_back({q, p, X, q, nullptr, 0, R, p, Tws});
+        cpR.push_back(cd2(R, Rc, p, p, p, 1, 1, p));          // Rc = R1^T
+        jac.push_back({p, p, Rc, p, nullptr, 0, sig, perm, info});
         tr.push_back({sig, perm, p, rank});
-        sel.push_back({W, p, sig, perm, rank, p, q, p, Wt, p, 0});
-        sel.push_back({Rc, p, sig, perm, rank, p, q, p, Bt, p, 0});
-        cpW.push_back(cd2(Wt, y->core(t, j), p, q, 1, p, yc, 1));
-        g2.push_back(gd(q, q, p, Q, 1, q, Bt, 1, p, T1, 1, q));
+        sel.push_back({Rc, p, sig, perm, rank, p, q, p, Vt, p, 1});
+        cpW.push_back(cd2(Vt, y->core(t, j), p, q, 1, p, yc, 1));
+        g2.push_back(gd(q, q, p, y->core(t, j), 1, yc, Vt, 1, p, T1, 1, q));   // M V (before core j changes)
       }
       g3.push_back(gd(ml, q, q, y->core(t, j - 1), 1, ml, T1, 1, q, T2, 1, ml));
       cpT2.push_back(cd2(T2, y->core(t, j - 1), ml, q, 1, ml, 1, ml));
@@ -176,9 +177,9 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
     B.jacobi(jac);
     B.trunc(tr, tol, rmax);
     B.select(sel);
+    B.gemm(g2);      // reads core j (p < q branch) before g1 / cpW overwrite it
     B.gemm(g1);
     B.copy(cpW);
-    B.gemm(g2);
     B.gemm(g3);
     B.copy(cpT2);
     B.release(mk);

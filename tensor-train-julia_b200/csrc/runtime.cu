@@ -79,7 +79,7 @@ static void launch_op(ttc_context* c, const Plan& p, const Op& op) {
     switch (op.kind) {
       case OP_GEMM: launch_gemm_f64((const GemmDesc*)d, op.count, op.total, s); break;
       case OP_QR: launch_qr((const QRDesc*)d, op.count, op.a, s, c->d_flags); break;
-      case OP_JACOBI: launch_jacobi((const JacobiDesc*)d, op.count, op.a, op.b, s, c->d_flags); break;
+      case OP_JACOBI: launch_jacobi((const JacobiDesc*)d, op.count, op.a, op.b, op.total != 0, s, c->d_flags); break;
       case OP_TRUNC: launch_truncate((const TruncDesc*)d, op.count, op.tol, op.rmax, s); break;
       case OP_SELECT: launch_select((const SelectDesc*)d, op.count, op.a, op.b, s); break;
       case OP_COPY: launch_copy((const CopyDesc*)d, op.count, op.total, s); break;
@@ -150,6 +150,19 @@ static void run_plan_profiled(ttc_context* c, Plan& p) {
     c->stats.kind_flops[kinds[j]] += flops[j];
   }
   for (auto e : ev) cudaEventDestroy(e);
+  // Jacobi sweep counters written into the plan blob
+  c->stats.jacobi_problems = 0; c->stats.jacobi_sweeps_sum = 0; c->stats.jacobi_sweeps_max = 0;
+  for (const auto& dg : p.diag) {
+    std::vector<int> v((size_t)dg.second);
+    TTC_CUDA(cudaMemcpy(v.data(), p.d_blob + dg.first, v.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int x : v) {
+      if (x == 0) continue;   // problem not run (empty)
+      const int sw = x < 0 ? -x : x;
+      c->stats.jacobi_problems += 1;
+      c->stats.jacobi_sweeps_sum += sw;
+      c->stats.jacobi_sweeps_max = std::max<int64_t>(c->stats.jacobi_sweeps_max, sw);
+    }
+  }
 }
 
 void run_plan(ttc_context* c, Plan& p) {
@@ -224,6 +237,11 @@ int* Builder::wi(size_t n) {
   wshw = std::max(wshw, wsoff);
   return reinterpret_cast<int*>(wsbase + o);
 }
+int* Builder::diag_ints(int n) {
+  const size_t o = plan->push(std::vector<int>((size_t)std::max(n, 1), 0));
+  plan->diag.push_back({o, std::max(n, 1)});
+  return reinterpret_cast<int*>(blob_base + o);
+}
 void Builder::stage(int id) {
   Op op; op.kind = OP_STAGE; op.a = id;
   plan->ops.push_back(op);
@@ -287,6 +305,7 @@ void Builder::jacobi(const std::vector<JacobiDesc>& v) {
     TTC_REQUIRE(2LL * 1 * (d.m + (d.W ? d.n : 0)) <= 25600 && d.n <= 25600, TTC_EDIM, "jacobi: matrix too large");
   }
   Op op; op.kind = OP_JACOBI; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm; op.b = nn;
+  for (auto& d : v) op.total |= (d.W != nullptr);
   for (auto& d : v) op.flops += 4.0 * d.m * (double)d.n * d.n + 8.0 * (double)d.n * d.n * d.n;
   plan->ops.push_back(op);
 }

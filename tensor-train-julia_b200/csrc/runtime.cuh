@@ -62,6 +62,7 @@ struct Plan {
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t graph_stream = nullptr;
   long long launches = 0;
+  std::vector<std::pair<size_t, int>> diag;   // (blob offset, count) of Jacobi sweep counters
   ~Plan();
   template <class T>
   size_t push(const std::vector<T>& v) {

@@ -1,26 +1,43 @@
-// Batched one-sided (Hestenes) Jacobi SVD, one CTA per problem, FP64.
+// Batched one-sided (Hestenes) Jacobi SVD, FP64, one thread-block cluster per problem.
 //
 // Replaces the LAPACK gesdd/gesvd call of the truncated-SVD sweep
 // (src/tt_rounding.jl:191-195, :235-239).  The sweep driver first QR-factors the
-// unfolding, so the Jacobi input is the small triangular factor R (one-sided Jacobi
-// preconditioned by QR converges in few sweeps and keeps singular values accurate to
-// O(eps * ||R||), the same backward-error level as LAPACK).
+// unfolding, so the Jacobi input is a small square factor (one-sided Jacobi preconditioned
+// by QR converges in few sweeps and keeps singular values accurate to O(eps * ||X||), the
+// backward-error level of LAPACK).
 //
-// Data movement: columns are split into blocks of bw (<= 32) columns.  A sweep keeps
-// block I in shared memory, rotates all pairs inside it, then streams every later block
-// J through a second shared-memory slot and rotates all (i in I, j in J) pairs.  During
-// that cross phase each warp keeps its own columns of block I in registers and only the
-// partner column of J moves through shared memory.  Every pair is visited once per sweep.
-// A sweep without any rotation above tol * sqrt(alpha*beta) ends the iteration.
+// Parallel block ordering.  Columns are split into nblk blocks of bw columns.  One sweep =
+// (a) the pairs inside every block, then (b) nblk'-1 rounds of the circle method over the
+// blocks (nblk' = nblk rounded up to even): in a round the block pairs are disjoint, so the
+// C CTAs of the cluster take them in turn, each streaming its two blocks from global memory
+// (L2-resident) into shared memory, rotating all b x b cross pairs and writing them back.
+// Rounds are separated by cluster barriers (barrier.cluster with release/acquire semantics,
+// which orders the global-memory writes of one CTA before the reads of the next round);
+// the "any rotation" flag of a sweep is OR-reduced into CTA 0's shared memory through
+// distributed shared memory.  Control flow is identical in every CTA of a cluster, so
+// every CTA reaches every barrier.
+//
+// Cross phase: each warp keeps its OWNT columns of the first block in registers, and only
+// the partner column of the second block moves through shared memory; the OWNT rotations
+// of a warp are independent and interleaved for instruction-level parallelism.
+//
+// Rotation (Rutishauser's formulas): with alpha = ||x||^2, beta = ||y||^2, gamma = x.y,
+// rotate when gamma^2 > tol^2 alpha beta; d = beta - alpha,
+// t = sign(d) 2 gamma / (|d| + sqrt(d^2 + 4 gamma^2)), c = 1/sqrt(1 + t^2), s = c t.
+// alpha, beta, gamma are scaled by a power of two that brings ||X||_F^2 into [1/4, 1], so
+// the squares cannot overflow or underflow (the rotation is scale invariant).
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
 #include "kernels.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace ttc {
 namespace {
 constexpr int NT = 256;
 constexpr int NW = NT / 32;
-constexpr int BWMAX = 32;
-constexpr int OWN = BWMAX / NW;     // columns of block I owned per warp (<= 4)
-constexpr int RPL = 16;             // register rows per lane in the cross phase (m <= 512)
 constexpr int MAX_SWEEPS = 40;
 // Rotation threshold |a_i.a_j| > tol * ||a_i|| ||a_j|| with tol = max(m, 16) eps, the worst-case
 // rounding error of an m-term FP64 dot product.  A threshold nearer the typical error
@@ -34,32 +51,36 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-struct Rot { double c, s; bool apply; bool big; };
+struct Rot { double c, s; bool apply; };
+
+// Parameters shared by all rotations of one problem.
+struct RotCfg {
+  double sc;     // power-of-two scale applied to alpha, beta, gamma
+  double tol2;   // tol^2
+  double zthr;   // scaled squared norm below which a column is numerically zero
+};
 
 // Columns whose squared norm is <= zthr (= (tol * ||A||_F)^2) are numerically zero: they are
 // left alone, as in LAPACK's dgesvj.  Without this rule a rank-deficient matrix (more columns
 // than the dimension of its column space) keeps rotating noise columns that cannot all be
 // mutually orthogonal, and the iteration never stops.
-__device__ __forceinline__ Rot make_rot(double alpha, double beta, double gamma, double tol, double zthr) {
-  Rot r{1.0, 0.0, false, false};
-  if (alpha <= zthr || beta <= zthr) return r;
-  const double ag = fabs(gamma);
-  const double lim = tol * sqrt(alpha) * sqrt(beta);
-  if (!(ag > lim)) return r;
-  r.big = true;
-  const double zeta = (beta - alpha) / (2.0 * gamma);
-  double t;
-  if (fabs(zeta) > 1e150) t = 0.5 / zeta;
-  else t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
-  r.c = 1.0 / sqrt(fma(t, t, 1.0));
+__device__ __forceinline__ Rot make_rot(double alpha, double beta, double gamma, const RotCfg& q) {
+  Rot r{1.0, 0.0, false};
+  alpha *= q.sc; beta *= q.sc; gamma *= q.sc;
+  if (alpha <= q.zthr || beta <= q.zthr) return r;
+  const double g2 = gamma * gamma;
+  if (!(g2 > q.tol2 * alpha * beta)) return r;
+  const double d = beta - alpha;
+  const double t = copysign(1.0, d) * (2.0 * gamma) / (fabs(d) + sqrt(fma(d, d, 4.0 * g2)));
+  r.c = rsqrt(fma(t, t, 1.0));
   r.s = r.c * t;
   r.apply = true;
   return r;
 }
 
-// Rotate columns x, y (both in shared memory, m rows) with one warp.  Returns whether a
-// rotation above the tolerance was applied.  W columns (n rows, shared) follow along.
-__device__ bool rotate_smem(double* x, double* y, int m, double* wx, double* wy, int n, double zthr) {
+// Rotate columns x, y (both in shared memory, m rows) with one warp.  W columns (n rows,
+// shared) follow along.  Returns whether a rotation was applied.
+__device__ bool rotate_smem(double* x, double* y, int m, double* wx, double* wy, int n, const RotCfg& q) {
   const int lane = threadIdx.x & 31;
   double a = 0.0, b = 0.0, g = 0.0;
   for (int r = lane; r < m; r += 32) {
@@ -67,7 +88,7 @@ __device__ bool rotate_smem(double* x, double* y, int m, double* wx, double* wy,
     a = fma(u, u, a); b = fma(v, v, b); g = fma(u, v, g);
   }
   a = warp_sum(a); b = warp_sum(b); g = warp_sum(g);
-  const Rot R = make_rot(a, b, g, jac_tol(m), zthr);
+  const Rot R = make_rot(a, b, g, q);
   if (!R.apply) return false;
   for (int r = lane; r < m; r += 32) {
     const double u = x[r], v = y[r];
@@ -80,20 +101,16 @@ __device__ bool rotate_smem(double* x, double* y, int m, double* wx, double* wy,
       wx[r] = R.c * u - R.s * v;
       wy[r] = fma(R.s, u, R.c * v);
     }
-  return R.big;
+  return true;
 }
 
-// Cross rotations between block I (in S0, cI columns) and block J (in S1, cJ columns).
-// Warp w owns the OWNT columns a = w + NW*o of block I in registers; in round s it rotates
-// a against b = (a + s) mod bw of block J.  The OWNT rotations of a warp are independent, so
-// their loads, dot products, shuffle reductions and updates are interleaved to hide the
-// latency chains (one rotation alone is latency bound).  Requires bw == NW*OWNT and
-// m <= 32*RPLT.  Returns whether a rotation above the threshold happened.
+// Cross rotations between block I (in S0, cI columns) and block J (in S1, cJ columns), both
+// of width bw = NW * OWNT.  Warp w owns the columns a = w + NW*o of block I in registers; in
+// step s it rotates a against b = (a + s) mod bw of block J.  Requires m <= 32 * RPLT.
 template <int OWNT, int RPLT>
-__device__ __forceinline__ int cross_regs(double* S0, double* S1, int m, int bw, int cI, int cJ, int warp, int lane,
-                                          double zthr) {
-  const int rpl = (m + 31) / 32;
-  const double tol = jac_tol(m);
+__device__ __forceinline__ bool cross_regs(double* S0, double* S1, int m, int cI, int cJ, const RotCfg& q) {
+  constexpr int bw = NW * OWNT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double xr[OWNT][RPLT];
 #pragma unroll
   for (int o = 0; o < OWNT; ++o) {
@@ -101,10 +118,10 @@ __device__ __forceinline__ int cross_regs(double* S0, double* S1, int m, int bw,
 #pragma unroll
     for (int t = 0; t < RPLT; ++t) {
       const int r = lane + 32 * t;
-      xr[o][t] = (a < cI && t < rpl && r < m) ? S0[a * m + r] : 0.0;
+      xr[o][t] = (a < cI && r < m) ? S0[a * m + r] : 0.0;
     }
   }
-  int any = 0;
+  bool any = false;
   for (int s = 0; s < bw; ++s) {
     double yr[OWNT][RPLT];
     double al[OWNT], be[OWNT], ga[OWNT];
@@ -119,7 +136,7 @@ __device__ __forceinline__ int cross_regs(double* S0, double* S1, int m, int bw,
 #pragma unroll
       for (int t = 0; t < RPLT; ++t) {
         const int r = lane + 32 * t;
-        yr[o][t] = (act[o] && t < rpl && r < m) ? y[r] : 0.0;
+        yr[o][t] = (act[o] && r < m) ? y[r] : 0.0;
       }
     }
 #pragma unroll
@@ -140,9 +157,9 @@ __device__ __forceinline__ int cross_regs(double* S0, double* S1, int m, int bw,
       }
 #pragma unroll
     for (int o = 0; o < OWNT; ++o) {
-      const Rot R = act[o] ? make_rot(al[o], be[o], ga[o], tol, zthr) : Rot{1.0, 0.0, false, false};
+      const Rot R = act[o] ? make_rot(al[o], be[o], ga[o], q) : Rot{1.0, 0.0, false};
       if (R.apply) {
-        any |= R.big;
+        any = true;
         const int a = warp + NW * o;
         double* y = S1 + ((a + s) % bw) * m;
 #pragma unroll
@@ -150,7 +167,7 @@ __device__ __forceinline__ int cross_regs(double* S0, double* S1, int m, int bw,
           const int r = lane + 32 * t;
           const double u = xr[o][t], v = yr[o][t];
           xr[o][t] = R.c * u - R.s * v;
-          if (t < rpl && r < m) y[r] = fma(R.s, u, R.c * v);
+          if (r < m) y[r] = fma(R.s, u, R.c * v);
         }
       }
     }
@@ -162,10 +179,45 @@ __device__ __forceinline__ int cross_regs(double* S0, double* S1, int m, int bw,
 #pragma unroll
     for (int t = 0; t < RPLT; ++t) {
       const int r = lane + 32 * t;
-      if (a < cI && t < rpl && r < m) S0[a * m + r] = xr[o][t];
+      if (a < cI && r < m) S0[a * m + r] = xr[o][t];
     }
   }
   return any;
+}
+
+// Cross rotations through shared memory only (W accumulation, or m beyond the register path).
+__device__ bool cross_smem(double* S0, double* S1, double* W0, double* W1, int m, int n, int bw, int cI, int cJ,
+                           const RotCfg& q) {
+  const int warp = threadIdx.x >> 5;
+  bool any = false;
+  for (int s = 0; s < bw; ++s) {
+    for (int a = warp; a < cI; a += NW) {
+      const int b = (a + s) % bw;
+      if (b < cJ)
+        any |= rotate_smem(S0 + a * m, S1 + b * m, m, W0 ? W0 + a * n : nullptr, W1 ? W1 + b * n : nullptr, n, q);
+    }
+    __syncthreads();
+  }
+  return any;
+}
+
+// Copy `cols` columns of `rows` doubles between global memory and shared memory (or back):
+// one warp per column, lanes over rows, four independent loads in flight per lane.
+__device__ __forceinline__ void copy_cols(double* __restrict__ dst, long long dld, const double* __restrict__ src,
+                                          long long sld, int rows, int cols) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = warp; c < cols; c += NW) {
+    const double* sc = src + (long long)c * sld;
+    double* dc = dst + (long long)c * dld;
+    for (int r0 = lane; r0 < rows; r0 += 128) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = (r0 + 32 * u < rows) ? sc[r0 + 32 * u] : 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (r0 + 32 * u < rows) dc[r0 + 32 * u] = v[u];
+    }
+  }
 }
 
 // Column position in the circle-method round robin over an even count `ne` of players.
@@ -173,134 +225,136 @@ __device__ __forceinline__ int rr_player(int pos, int round, int ne) {
   if (pos == 0) return 0;
   return ((pos - 1 + round) % (ne - 1)) + 1;
 }
+
+// Register-path dispatch on the rows per lane (bw = 16: two own columns per warp), up to
+// RMAX rows per lane.
+template <int RMAX>
+__device__ bool cross_dispatch(double* S0, double* S1, int m, int cI, int cJ, const RotCfg& q) {
+  const int rpl = (m + 31) / 32;
+  if (rpl <= 2) return cross_regs<2, 2>(S0, S1, m, cI, cJ, q);
+  if (rpl <= 4) return cross_regs<2, 4>(S0, S1, m, cI, cJ, q);
+  if (RMAX <= 8 || rpl <= 8) return cross_regs<2, (RMAX < 8 ? RMAX : 8)>(S0, S1, m, cI, cJ, q);
+  return cross_regs<2, RMAX>(S0, S1, m, cI, cJ, q);
+}
 }  // namespace
 
-__global__ void __launch_bounds__(NT, 1) jacobi_svd_kernel(const JacobiDesc* __restrict__ descs, int smem_doubles,
-                                                           int* flags) {
+// grid = count * csize CTAs, clusters of csize CTAs (one cluster per problem).  RMAX bounds
+// the register rows per lane of the cross phase (m <= 32 RMAX); RMAX = 8 keeps the kernel
+// within 128 registers so that two CTAs share an SM.
+template <int RMAX>
+__global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
+    jacobi_svd_kernel(const JacobiDesc* __restrict__ descs, int bw, int csize, int* flags) {
   extern __shared__ double sm[];
-  __shared__ int s_rot;
-  const JacobiDesc D = descs[blockIdx.x];
+  __shared__ int s_any;
+  __shared__ double s_red[NW];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int crank = (int)cluster.block_rank();
+  const JacobiDesc D = descs[blockIdx.x / csize];
   const int m = D.m, n = D.n;
-  if (m <= 0 || n <= 0) return;
+  if (m <= 0 || n <= 0) return;                 // uniform across the cluster
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool accw = (D.W != nullptr);
-  // block width: largest power of two <= 32 whose two slots fit
-  int bw = BWMAX;
-  if (!accw && m > 256) bw = 16;     // register cross phase: 2 own columns x 16 rows per lane
-  while (bw > 1 && 2LL * bw * (m + (accw ? n : 0)) > smem_doubles) bw >>= 1;
   const int nblk = (n + bw - 1) / bw;
+  const int ne = nblk + (nblk & 1);
   double* S0 = sm;
   double* S1 = sm + (size_t)bw * m;
   double* W0 = S1 + (size_t)bw * m;
   double* W1 = W0 + (accw ? (size_t)bw * n : 0);
-  const bool use_regs = !accw && ((bw == 32 && m <= 256) || (bw == 16 && m <= 512));
+  const bool use_regs = !accw && bw == 16 && m <= 32 * RMAX;
 
-  if (accw) {  // W = I
-    for (long long e = tid; e < (long long)n * n; e += NT) {
+  if (accw) {  // W = I (columns split over the cluster)
+    for (long long e = tid + (long long)crank * NT; e < (long long)n * n; e += (long long)NT * csize) {
       const int j = (int)(e / n), i = (int)(e - (long long)j * n);
       D.W[(long long)j * D.ldw + i] = (i == j) ? 1.0 : 0.0;
     }
   }
-  // ||X||_F^2 (invariant under the rotations) -> numerical-zero threshold for columns
-  __shared__ double s_red[NW];
+  // ||X||_F^2 (invariant under the rotations): scale and numerical-zero threshold
   {
     double a = 0.0;
-    for (long long e = tid; e < (long long)m * n; e += NT) {
-      const int j = (int)(e / m), i = (int)(e - (long long)j * m);
-      const double v = D.X[(long long)j * D.ldx + i];
-      a = fma(v, v, a);
+    for (int j = warp; j < n; j += NW) {
+      const double* xc = D.X + (long long)j * D.ldx;
+      for (int i = lane; i < m; i += 32) a = fma(xc[i], xc[i], a);
     }
     a = warp_sum(a);
     if (lane == 0) s_red[warp] = a;
   }
+  if (tid == 0) s_any = 0;
   __syncthreads();
   double fro2 = 0.0;
 #pragma unroll
   for (int i = 0; i < NW; ++i) fro2 += s_red[i];
-  const double zt = jac_tol(m);
-  const double zthr = zt * zt * fro2;
-  __syncthreads();
+  RotCfg q;
+  {
+    const double tol = jac_tol(m);
+    int e2 = 0;
+    if (fro2 > 0.0 && isfinite(fro2)) { frexp(fro2, &e2); e2 = (e2 + 1) & ~1; }   // even exponent
+    q.sc = (fro2 > 0.0 && isfinite(fro2)) ? ldexp(1.0, -e2) : 1.0;
+    q.tol2 = tol * tol;
+    q.zthr = q.tol2 * fro2 * q.sc;
+  }
 
   auto load_block = [&](int blk, double* S, double* Wd) {
     const int c0 = blk * bw, cn = min(bw, n - c0);
-    for (int e = tid; e < cn * m; e += NT) {
-      const int c = e / m, r = e - c * m;
-      S[c * m + r] = D.X[(long long)(c0 + c) * D.ldx + r];
-    }
-    if (accw)
-      for (int e = tid; e < cn * n; e += NT) {
-        const int c = e / n, r = e - c * n;
-        Wd[c * n + r] = D.W[(long long)(c0 + c) * D.ldw + r];
-      }
+    copy_cols(S, m, D.X + (long long)c0 * D.ldx, D.ldx, m, cn);
+    if (accw) copy_cols(Wd, n, D.W + (long long)c0 * D.ldw, D.ldw, n, cn);
   };
   auto store_block = [&](int blk, const double* S, const double* Wd) {
     const int c0 = blk * bw, cn = min(bw, n - c0);
-    for (int e = tid; e < cn * m; e += NT) {
-      const int c = e / m, r = e - c * m;
-      D.X[(long long)(c0 + c) * D.ldx + r] = S[c * m + r];
-    }
-    if (accw)
-      for (int e = tid; e < cn * n; e += NT) {
-        const int c = e / n, r = e - c * n;
-        D.W[(long long)(c0 + c) * D.ldw + r] = Wd[c * n + r];
-      }
+    copy_cols(D.X + (long long)c0 * D.ldx, D.ldx, S, m, m, cn);
+    if (accw) copy_cols(D.W + (long long)c0 * D.ldw, D.ldw, Wd, n, n, cn);
   };
+  cluster.sync();   // W = I visible to every CTA
 
+  int* any0 = cluster.map_shared_rank(&s_any, 0);
   bool converged = false;
   int sweep = 0;
   for (; sweep < MAX_SWEEPS && !converged; ++sweep) {
-    if (tid == 0) s_rot = 0;
-    __syncthreads();
-    int any = 0;
-    for (int I = 0; I < nblk; ++I) {
-      const int cI = min(bw, n - I * bw);
-      if (nblk > 1 || sweep == 0) { load_block(I, S0, W0); }
+    bool any = false;
+    // (a) pairs inside each block; blocks dealt to the CTAs of the cluster
+    for (int blk = crank; blk < nblk; blk += csize) {
+      const int cI = min(bw, n - blk * bw);
+      load_block(blk, S0, W0);
       __syncthreads();
-      // intra-block pairs: circle method over an even number of players
-      {
-        const int ne = cI + (cI & 1);
-        for (int rd = 0; rd < ne - 1; ++rd) {
-          for (int p = warp; p < ne / 2; p += NW) {
-            const int i = rr_player(p, rd, ne), j = rr_player(ne - 1 - p, rd, ne);
-            if (i < cI && j < cI)
-              any |= rotate_smem(S0 + i * m, S0 + j * m, m, accw ? W0 + i * n : nullptr,
-                                 accw ? W0 + j * n : nullptr, n, zthr);
-          }
-          __syncthreads();
-        }
-      }
-      // cross pairs with every later block
-      for (int J = I + 1; J < nblk; ++J) {
-        const int cJ = min(bw, n - J * bw);
-        load_block(J, S1, W1);
-        __syncthreads();
-        if (use_regs) {
-          if (bw == 32) any |= cross_regs<4, 8>(S0, S1, m, bw, cI, cJ, warp, lane, zthr);
-          else any |= cross_regs<2, 16>(S0, S1, m, bw, cI, cJ, warp, lane, zthr);
-        } else {
-          for (int s = 0; s < bw; ++s) {
-            for (int a = warp; a < cI; a += NW) {
-              const int b = (a + s) % bw;
-              if (b < cJ)
-                any |= rotate_smem(S0 + a * m, S1 + b * m, m, accw ? W0 + a * n : nullptr,
-                                   accw ? W1 + b * n : nullptr, n, zthr);
-            }
-            __syncthreads();
-          }
+      const int nee = cI + (cI & 1);
+      for (int rd = 0; rd < nee - 1; ++rd) {
+        for (int p = warp; p < nee / 2; p += NW) {
+          const int i = rr_player(p, rd, nee), j = rr_player(nee - 1 - p, rd, nee);
+          if (i < cI && j < cI)
+            any |= rotate_smem(S0 + i * m, S0 + j * m, m, accw ? W0 + i * n : nullptr, accw ? W0 + j * n : nullptr,
+                               n, q);
         }
         __syncthreads();
-        store_block(J, S1, W1);
-        __syncthreads();
       }
-      if (nblk > 1) store_block(I, S0, W0);
+      store_block(blk, S0, W0);
       __syncthreads();
     }
-    if (any && lane == 0) atomicOr(&s_rot, 1);
-    __syncthreads();
-    converged = (s_rot == 0);
-    __syncthreads();
+    cluster.sync();
+    // (b) cross pairs: circle method over the blocks, disjoint pairs per round
+    for (int rd = 0; rd < ne - 1; ++rd) {
+      for (int p = crank; p < ne / 2; p += csize) {
+        const int bi = rr_player(p, rd, ne), bj = rr_player(ne - 1 - p, rd, ne);
+        if (bi >= nblk || bj >= nblk) continue;
+        const int cI = min(bw, n - bi * bw), cJ = min(bw, n - bj * bw);
+        load_block(bi, S0, W0);
+        load_block(bj, S1, W1);
+        __syncthreads();
+        if (use_regs) any |= cross_dispatch<RMAX>(S0, S1, m, cI, cJ, q);
+        else any |= cross_smem(S0, S1, accw ? W0 : nullptr, accw ? W1 : nullptr, m, n, bw, cI, cJ, q);
+        __syncthreads();
+        store_block(bi, S0, W0);
+        store_block(bj, S1, W1);
+        __syncthreads();
+      }
+      cluster.sync();
+    }
+    // OR of the per-CTA flags into CTA 0; every CTA reads it; CTA 0 clears it for the next sweep
+    if (any && lane == 0) atomicOr(any0, 1);
+    cluster.sync();
+    converged = (*any0 == 0);
+    cluster.sync();
+    if (crank == 0 && tid == 0) s_any = 0;
   }
-  if (nblk == 1) { store_block(0, S0, W0); __syncthreads(); }
+  if (crank != 0) return;   // no distributed-shared-memory access follows
   if (!converged && tid == 0) atomicOr(flags, DFLAG_JACOBI_NOCONV);
   if (D.info && tid == 0) *D.info = converged ? sweep : -sweep;
 
@@ -324,17 +378,82 @@ __global__ void __launch_bounds__(NT, 1) jacobi_svd_kernel(const JacobiDesc* __r
   }
 }
 
-void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, cudaStream_t s, int* d_flags) {
-  if (count <= 0) return;
-  (void)max_m; (void)max_n;
-  const int smem_bytes = 200 * 1024;
-  static bool attr_set = false;
-  if (!attr_set) {
-    TTC_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes));
-    attr_set = true;
+namespace {
+int sm_count() {
+  static int dev_cached = -1, count = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev != dev_cached) {
+    TTC_CUDA(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev));
+    dev_cached = dev;
   }
-  jacobi_svd_kernel<<<count, NT, smem_bytes, s>>>(d_descs, smem_bytes / (int)sizeof(double), d_flags);
+  return count;
+}
+}  // namespace
+
+// Block width and dynamic shared memory of a launch: two blocks of bw columns (and their W
+// columns), at least n doubles for the final singular-value pass.
+static int jacobi_bw(int max_m, int max_n, bool accw, size_t* smem_out) {
+  int bw = 16;
+  auto need = [&](int b) {
+    return sizeof(double) * std::max<size_t>(2 * (size_t)b * (max_m + (accw ? max_n : 0)), (size_t)max_n);
+  };
+  while (bw > 1 && need(bw) > 200 * 1024) bw >>= 1;
+  *smem_out = need(bw);
+  return bw;
+}
+
+template <int RMAX>
+static int jacobi_cluster_size(int count, int max_n, int bw, size_t smem) {
+  // CTAs per problem: fill the SMs (resident CTAs per SM from registers and shared memory),
+  // at most 8 (portable cluster size) and at most the disjoint block pairs of a round.
+  int per_sm = 1;
+  TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_svd_kernel<RMAX>, NT, smem));
+  per_sm = std::max(1, per_sm);
+  const int slots = sm_count() * per_sm;
+  const int pairs = std::max(1, ((max_n + bw - 1) / bw + 1) / 2);
+  int c = std::max(1, slots / std::max(1, count));
+  c = std::min(c, std::min(8, pairs));
+  int p2 = 1;
+  while (p2 * 2 <= c) p2 *= 2;
+  return p2;
+}
+
+template <int RMAX>
+static void launch_jacobi_t(const JacobiDesc* d_descs, int count, int max_n, int bw, size_t smem, cudaStream_t s,
+                            int* d_flags) {
+  static int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    TTC_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel<RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr_dev = dev;
+  }
+  const int csize = jacobi_cluster_size<RMAX>(count, max_n, bw, smem);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)(count * csize));
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)csize;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  TTC_CUDA(cudaLaunchKernelEx(&cfg, jacobi_svd_kernel<RMAX>, d_descs, bw, csize, d_flags));
   TTC_CHECK_LAUNCH();
+}
+
+void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, bool accw, cudaStream_t s,
+                   int* d_flags) {
+  if (count <= 0) return;
+  size_t smem = 0;
+  const int bw = jacobi_bw(max_m, max_n, accw, &smem);
+  TTC_REQUIRE(smem <= 200 * 1024, TTC_EDIM, "jacobi: matrix too large for the shared-memory blocks");
+  if (max_m <= 256) launch_jacobi_t<8>(d_descs, count, max_n, bw, smem, s, d_flags);
+  else launch_jacobi_t<16>(d_descs, count, max_n, bw, smem, s, d_flags);
 }
 
 }  // namespace ttc
