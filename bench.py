@@ -148,7 +148,7 @@ def cpu_reference_rate(dims, tts, rks, sample):
     t0 = time.perf_counter()
     for dims_i, r, vec in tts[:sample]:
         x = o.TTvector(len(dims_i), [c.copy() for c in vec], tuple(dims_i), list(r), [0] * len(dims_i))
-        y = o.ttrand_rounding(x, rks, orthogonal=False, seed=1234, block_rks=max(rks))
+        y = o.ttrand_rounding(x, rks, orthogonal=True, seed=1234, block_rks=len(dims_i))
         o.tt_rounding(y, tol=TOL)
     dt = time.perf_counter() - t0
     return sample / dt, dt
@@ -222,7 +222,7 @@ def main():
     ranks = [r for _, r, _ in tts]
     tt_objs = [ttcuda.TTvector(len(d_), v, d_, r, [0] * len(d_)) for d_, r, v in tts]
     rks = heuristic(ranks)
-    block = max(rks)
+    block = D                        # ttrand_rounding's default block_rks = N
     s = ttcuda._sketch_ranks(dims, rks, block)
     rho = ttcuda._rand_out_caps(dims, s)
     xb = ttcuda.DeviceBatch.from_tts(tt_objs, ctx=ctx)
@@ -230,7 +230,7 @@ def main():
     y_fp64 = ttcuda.DeviceBatch(dims, ranks, ctx=ctx)
 
     def step_mixed(sync=False):
-        xb.round_rand(y_mixed, rks, orthogonal=False, seed=1234, block_rks=block, precision="bf16",
+        xb.round_rand(y_mixed, rks, orthogonal=True, seed=1234, block_rks=block, precision="bf16",
                       after_tol=TOL, sync=sync)
 
     def step_fp64(sync=False):
@@ -362,7 +362,8 @@ def main():
             "config": {"workload": f"batched rounding: {len(tts)} TTs per GPU, d=32, n=2, ranks U[16,256] (seeded), "
                                    "sigma 10^(-i/32), tol 1e-8",
                        "variant": "mixed: BF16-sketch (tcgen05) ttrand_rounding + FP64 SVD sweep",
-                       "sketch_ranks": "default_rank_heuristic (r + ceil(max r/2)), block_rks = max",
+                       "sketch_ranks": "default_rank_heuristic of the batch (r + ceil(max r/2)); block_rks = N, "
+                                       "orthogonal blocks, seed 1234 (ttrand_rounding defaults)",
                        "l2": f"inputs {in_bytes / 1e6:.0f} MB resident > 126 MB L2"},
             "fp64": {"value": fp64_value, "unit": "roundings/s", "ms_per_step": ms_fp64 / args.steps,
                      "variant": "deterministic tt_rounding (FP64 Householder QR sweep + Jacobi SVD sweep)"},

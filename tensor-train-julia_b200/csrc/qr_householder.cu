@@ -14,9 +14,10 @@
 // backwards from the stored panels (dorgqr).
 //
 // One thread-block cluster of C CTAs per problem.  Every CTA factors each panel itself
-// (same data, same arithmetic: identical reflectors, no broadcast needed); the column pairs
-// (2p, 2p+1) of the trailing update and of Q are owned by CTA p mod C, so a column is always
-// updated by the same CTA.  A cluster barrier (release/acquire at cluster scope) after each
+// (same data, same arithmetic: identical reflectors, no broadcast needed); the column octets
+// (8o .. 8o+7) of the trailing update and of Q are owned by CTA o mod C, so a column is always
+// updated by the same CTA.  The block reflectors are applied on the FP64 tensor cores
+// (mma.sync m8n8k4).  A cluster barrier (release/acquire at cluster scope) after each
 // panel's trailing update makes the next panel visible to every CTA.  CTA 0 writes the
 // factored panels and the T factors, which the Q formation reads after one more barrier.
 #include <cooperative_groups.h>
@@ -73,83 +74,85 @@ __device__ __forceinline__ bool copy_cols(double* __restrict__ dst, long long dl
   return bad;
 }
 
+// D += A B on the FP64 tensor-core path (mma.sync m8n8k4): per lane a = A[lane>>2][lane&3],
+// b = B[lane&3][lane>>2], d = D[lane>>2][2(lane&3) + {0,1}].
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Reflector entry V[l][r] of the panel (unit diagonal and zeros above it implied).
+__device__ __forceinline__ double vref(const double* V, int mp_ld, int jb, int mp, int l, int r) {
+  if (l >= jb || r >= mp || r < l) return 0.0;
+  return (r == l) ? 1.0 : V[l * mp_ld + r];
+}
+
 // Apply (I - V T^T V^T) [trans=1] or (I - V T V^T) [trans=0] to columns [c_begin, c_end) of
 // the global matrix M (rows r0..m-1, ld), with V (mp x jb) in shared memory (column-major,
-// stride mp_ld, unit diagonal implied, zeros above) and T (jb x jb) in shared memory.
-// Column pairs (2p, 2p+1) with p mod csize == crank belong to this CTA.
+// stride mp_ld = 4 mod 16 for conflict-free fragment loads) and T (jb x jb) in shared memory.
+// One warp per octet of 8 columns; octet o belongs to CTA o mod csize.  Both products run on
+// the FP64 tensor cores: W (16 x 8) = V^T C accumulated over 4-row steps, U = T^T W (or T W)
+// through a per-warp scratch Ws (16 x 8), then C -= V U per 8-row tile.
 __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_begin, int c_end,
                                       const double* V, int mp_ld, int jb, const double* T, bool trans,
-                                      int crank, int csize) {
+                                      int crank, int csize, double* Wscr) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qr = lane >> 2, qc = lane & 3;
   const int mp = m - r0;
-  const int p_begin = c_begin >> 1, p_end = (c_end + 1) >> 1;
-  const int p_first = p_begin + ((crank - p_begin) % csize + csize) % csize;
-  for (int p = p_first + warp * csize; p < p_end; p += NW * csize) {
-    const int c = 2 * p;
-    if (c + 1 < c_begin) continue;
-    // a pair may straddle c_begin (odd start) or c_end: update only the columns inside
-    const bool has0 = (c >= c_begin), two = has0 ? (c + 1 < c_end) : false;
-    double* col0 = M + (long long)(has0 ? c : c + 1) * ld + r0;
-    double* col1 = M + (long long)(c + 1) * ld + r0;
-    double w0[NB], w1[NB];
-#pragma unroll
-    for (int l = 0; l < NB; ++l) { w0[l] = 0.0; w1[l] = 0.0; }
+  double* Ws = Wscr + warp * 128;
+  const int o_begin = c_begin >> 3, o_end = (c_end + 7) >> 3;
+  const int o_first = o_begin + ((crank - o_begin) % csize + csize) % csize;
+  for (int o = o_first + warp * csize; o < o_end; o += NW * csize) {
+    const int c0 = 8 * o;
+    // pass 1: W = V^T C; B fragment = C[r][c0 + qr]
+    const int cb = c0 + qr;
+    const bool cb_ok = (cb >= c_begin && cb < c_end);
+    const double* colb = M + (long long)(cb_ok ? cb : c_begin) * ld + r0;
+    double w00 = 0.0, w01 = 0.0, w10 = 0.0, w11 = 0.0;
 #pragma unroll 4
-    for (int r = lane; r < mp; r += 32) {
-      const double x0 = col0[r];
-      const double x1 = two ? col1[r] : 0.0;
-#pragma unroll
-      for (int l = 0; l < NB; ++l) {
-        if (l < jb) {
-          const double v = (r > l) ? V[l * mp_ld + r] : (r == l ? 1.0 : 0.0);
-          w0[l] = fma(v, x0, w0[l]);
-          w1[l] = fma(v, x1, w1[l]);
-        }
-      }
+    for (int k0 = 0; k0 < mp; k0 += 4) {
+      const int r = k0 + qc;
+      const double b = (cb_ok && r < mp) ? colb[r] : 0.0;
+      dmma(w00, w01, vref(V, mp_ld, jb, mp, qr, r), b);
+      dmma(w10, w11, vref(V, mp_ld, jb, mp, 8 + qr, r), b);
     }
+    Ws[qr * 8 + 2 * qc] = w00;
+    Ws[qr * 8 + 2 * qc + 1] = w01;
+    Ws[(8 + qr) * 8 + 2 * qc] = w10;
+    Ws[(8 + qr) * 8 + 2 * qc + 1] = w11;
+    __syncwarp();
+    // U = T^T W or T W (T upper triangular); this lane needs -U[4s + qc][qr], s = 0..3
+    double ub[4];
 #pragma unroll
-    for (int l = 0; l < NB; ++l) {
-      if (l < jb) { w0[l] = warp_sum(w0[l]); w1[l] = warp_sum(w1[l]); }
+    for (int sidx = 0; sidx < 4; ++sidx) {
+      const int l = 4 * sidx + qc;
+      double u = 0.0;
+      if (l < jb) {
+        if (trans) {
+          for (int i = 0; i <= l; ++i) u = fma(T[l * NB + i], Ws[i * 8 + qr], u);
+        } else {
+          for (int i = l; i < jb; ++i) u = fma(T[i * NB + l], Ws[i * 8 + qr], u);
+        }
+      }
+      ub[sidx] = -u;
     }
-    // u = T^T w (trans) or T w, T upper triangular, computed in place: u_l = sum_{i<=l}
-    // T[i,l] w_i needs only w_0..w_l (descending l); u_l = sum_{i>=l} T[l,i] w_i needs only
-    // w_l..w_{jb-1} (ascending l).
-    if (trans) {
+    __syncwarp();   // Ws is rewritten for the next octet
+    // pass 2: C[rt..rt+7][c0..c0+7] -= V[rt.., 0..15] U
+    const int ca = c0 + 2 * qc;
+    const bool ok0 = (ca >= c_begin && ca < c_end), ok1 = (ca + 1 >= c_begin && ca + 1 < c_end);
+    double* col0 = M + (long long)(ok0 ? ca : c_begin) * ld + r0;
+    double* col1 = M + (long long)(ok1 ? ca + 1 : c_begin) * ld + r0;
+#pragma unroll 2
+    for (int rt = 0; rt < mp; rt += 8) {
+      const int r = rt + qr;
+      const bool rok = r < mp;
+      double d0 = (ok0 && rok) ? col0[r] : 0.0;
+      double d1 = (ok1 && rok) ? col1[r] : 0.0;
 #pragma unroll
-      for (int l = NB - 1; l >= 0; --l) {
-        double a0 = 0.0, a1 = 0.0;
-        if (l < jb) {
-#pragma unroll
-          for (int i = 0; i < NB; ++i)
-            if (i <= l) { a0 = fma(T[l * NB + i], w0[i], a0); a1 = fma(T[l * NB + i], w1[i], a1); }
-        }
-        w0[l] = a0; w1[l] = a1;
-      }
-    } else {
-#pragma unroll
-      for (int l = 0; l < NB; ++l) {
-        double a0 = 0.0, a1 = 0.0;
-        if (l < jb) {
-#pragma unroll
-          for (int i = 0; i < NB; ++i)
-            if (i >= l && i < jb) { a0 = fma(T[i * NB + l], w0[i], a0); a1 = fma(T[i * NB + l], w1[i], a1); }
-        }
-        w0[l] = a0; w1[l] = a1;
-      }
-    }
-#pragma unroll 4
-    for (int r = lane; r < mp; r += 32) {
-      double d0 = 0.0, d1 = 0.0;
-#pragma unroll
-      for (int l = 0; l < NB; ++l) {
-        if (l < jb) {
-          const double v = (r > l) ? V[l * mp_ld + r] : (r == l ? 1.0 : 0.0);
-          d0 = fma(v, w0[l], d0);
-          d1 = fma(v, w1[l], d1);
-        }
-      }
-      col0[r] -= d0;
-      if (two) col1[r] -= d1;
+      for (int sidx = 0; sidx < 4; ++sidx) dmma(d0, d1, vref(V, mp_ld, jb, mp, 4 * sidx + qc, r), ub[sidx]);
+      if (ok0 && rok) col0[r] = d0;
+      if (ok1 && rok) col1[r] = d1;
     }
   }
 }
@@ -167,8 +170,12 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
   double* T = sm;                    // NB*NB
   double* tau = T + NB * NB;         // NB
   double* red = tau + NB;            // NW
-  double* G = red + NW;              // NB*NB  (V^T V)
-  double* P = G + NB * NB;           // panel, (mp_ld x NB)
+  double* sv = red + NW;             // NB   reflector scales 1/(alpha - beta)
+  double* bet = sv + NB;             // NB   betas (diagonal of R)
+  double* nrm2 = bet + NB;           // 2    squared norm below the diagonal of the next column
+  double* G = nrm2 + 2;              // NB*NB  (V^T V)
+  double* Wscr = G + NB * NB;        // NW*128  per-warp 16 x 8 scratch of the reflector products
+  double* P = Wscr + NW * 128;       // panel, (mp_ld x NB), mp_ld = 4 mod 16
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   double* A = D.A;
   const int lda = D.lda;
@@ -177,15 +184,24 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
   for (int j0 = 0; j0 < K; j0 += NB) {
     const int jb = min(NB, K - j0);
     const int mp = m - j0;
-    const int mp_ld = mp;
+    const int mp_ld = mp + ((4 - mp) & 15);
     // 1. load panel
     nonfinite |= copy_cols(P, mp_ld, A + (long long)j0 * lda + j0, lda, mp, jb);
     __syncthreads();
-    // 2. factor panel
+    // 2. factor panel, one CTA barrier per column: reflector jj (dlarfg: beta =
+    //    -sign(alpha) ||(alpha, x)||, tau = (beta - alpha)/beta, v = [1; x/(alpha - beta)]) is
+    //    applied to columns c > jj with x unscaled; the warp that updates column jj+1 also
+    //    returns its squared norm below the diagonal for the next reflector.  The reflector
+    //    columns are scaled, and the betas stored, after the loop.
+    {
+      double s0 = 0.0;
+      for (int r = 1 + tid; r < mp; r += NT) { const double x = P[r]; s0 = fma(x, x, s0); }
+      s0 = block_sum(s0, red);
+      if (tid == 0) nrm2[0] = s0;
+      __syncthreads();
+    }
     for (int jj = 0; jj < jb; ++jj) {
-      double s = 0.0;
-      for (int r = jj + 1 + tid; r < mp; r += NT) { const double x = P[jj * mp_ld + r]; s = fma(x, x, s); }
-      s = block_sum(s, red);
+      const double s = nrm2[jj & 1];
       const double alpha = P[jj * mp_ld + jj];
       double beta, t, scal;
       if (s == 0.0) { t = 0.0; beta = alpha; scal = 0.0; }
@@ -194,27 +210,39 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
         t = (beta - alpha) / beta;
         scal = 1.0 / (alpha - beta);
       }
-      __syncthreads();
-      if (s != 0.0)
-        for (int r = jj + 1 + tid; r < mp; r += NT) P[jj * mp_ld + r] *= scal;
-      if (tid == 0) { P[jj * mp_ld + jj] = beta; tau[jj] = t; }
-      __syncthreads();
-      // apply H_jj to the remaining panel columns (one warp per column)
+      const double* x = P + jj * mp_ld;
       for (int c = jj + 1 + warp; c < jb; c += NW) {
-        double w = 0.0;
-        for (int r = jj + lane; r < mp; r += 32) {
-          const double v = (r == jj) ? 1.0 : P[jj * mp_ld + r];
-          w = fma(v, P[c * mp_ld + r], w);
+        double* pc = P + c * mp_ld;
+        const double cj = pc[jj];
+        double d = 0.0;
+        for (int r = jj + 1 + lane; r < mp; r += 32) d = fma(x[r], pc[r], d);
+        d = warp_sum(d);
+        const double w = fma(scal, d, cj) * t;     // tau v^T c
+        const double ws = w * scal;
+        double q = 0.0;
+        for (int r = jj + 1 + lane; r < mp; r += 32) {
+          const double u = fma(-ws, x[r], pc[r]);
+          pc[r] = u;
+          if (r > jj + 1) q = fma(u, u, q);
         }
-        w = warp_sum(w) * t;
-        for (int r = jj + lane; r < mp; r += 32) {
-          const double v = (r == jj) ? 1.0 : P[jj * mp_ld + r];
-          P[c * mp_ld + r] -= w * v;
+        if (c == jj + 1) {
+          q = warp_sum(q);
+          if (lane == 0) nrm2[(jj + 1) & 1] = q;
         }
+        if (lane == 0) pc[jj] = cj - w;
       }
+      if (tid == 0) { tau[jj] = t; sv[jj] = scal; bet[jj] = beta; }
       __syncthreads();
     }
-    // 3. T factor (dlarft, forward columnwise): G = V^T V, then T
+    for (int c = warp; c < jb; c += NW) {
+      double* pc = P + c * mp_ld;
+      const double sc = sv[c];
+      for (int r = c + 1 + lane; r < mp; r += 32) pc[r] *= sc;
+      if (lane == 0) pc[c] = bet[c];
+    }
+    __syncthreads();
+    // 3. T factor (dlarft, forward columnwise): G = V^T V by all warps, then T by one warp:
+    //    T[0:i, i] = -tau_i T[0:i, 0:i] G[0:i, i], T[i, i] = tau_i
     for (int pidx = warp; pidx < jb * jb; pidx += NW) {
       const int i = pidx / jb, l = pidx - i * jb;     // G[l][i] for l < i
       if (l < i) {
@@ -229,22 +257,21 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
       }
     }
     __syncthreads();
-    if (tid == 0) {
-      for (int i = 0; i < NB; ++i)
-        for (int l = 0; l < NB; ++l) T[i * NB + l] = 0.0;
+    if (warp == 0) {
+      for (int e = lane; e < NB * NB; e += 32) T[e] = 0.0;
+      __syncwarp();
       for (int i = 0; i < jb; ++i) {
-        T[i * NB + i] = tau[i];
-        // T[0:i, i] = -tau_i * T[0:i, 0:i] * G[0:i, i]
-        for (int r = 0; r < i; ++r) {
-          double a = 0.0;
-          for (int l = r; l < i; ++l) a = fma(T[l * NB + r], G[i * NB + l], a);
-          T[i * NB + r] = -tau[i] * a;
-        }
+        double a = 0.0;
+        if (lane < i)
+          for (int l = lane; l < i; ++l) a = fma(T[l * NB + lane], G[i * NB + l], a);
+        if (lane < i) T[i * NB + lane] = -tau[i] * a;
+        if (lane == i) T[i * NB + i] = tau[i];
+        __syncwarp();
       }
     }
     __syncthreads();
-    // 4. trailing update with H^T = I - V T^T V^T (this CTA's column pairs)
-    if (j0 + jb < n) apply_block_reflector(A, lda, j0, m, j0 + jb, n, P, mp_ld, jb, T, true, crank, csize);
+    // 4. trailing update with H^T = I - V T^T V^T (this CTA's column octets)
+    if (j0 + jb < n) apply_block_reflector(A, lda, j0, m, j0 + jb, n, P, mp_ld, jb, T, true, crank, csize, Wscr);
     // 5. CTA 0 writes back the panel and keeps T
     if (crank == 0) {
       copy_cols(A + (long long)j0 * lda + j0, lda, P, mp_ld, mp, jb);
@@ -263,19 +290,19 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
   }
   if (!D.Q) return;
   // Q = H_1 ... H_K [I; 0], accumulated backwards panel by panel.  Each CTA initialises
-  // and updates only its own column pairs, so the panels need no barrier between them.
+  // and updates only its own column octets, so the panels need no barrier between them.
   for (int c = 0; c < K; ++c) {
-    if (((c >> 1) % csize) != crank) continue;
+    if (((c >> 3) % csize) != crank) continue;
     for (int i = tid; i < m; i += NT) D.Q[(long long)c * D.ldq + i] = (i == c) ? 1.0 : 0.0;
   }
   __syncthreads();
   const int npan = (K + NB - 1) / NB;
   for (int p = npan - 1; p >= 0; --p) {
-    const int j0 = p * NB, jb = min(NB, K - j0), mp = m - j0, mp_ld = mp;
+    const int j0 = p * NB, jb = min(NB, K - j0), mp = m - j0, mp_ld = mp + ((4 - mp) & 15);
     copy_cols(P, mp_ld, A + (long long)j0 * lda + j0, lda, mp, jb);
     for (int e = tid; e < NB * NB; e += NT) T[e] = D.Tws[p * NB * NB + e];
     __syncthreads();
-    apply_block_reflector(D.Q, D.ldq, j0, m, j0, K, P, mp_ld, jb, T, false, crank, csize);
+    apply_block_reflector(D.Q, D.ldq, j0, m, j0, K, P, mp_ld, jb, T, false, crank, csize, Wscr);
     __syncthreads();
   }
 }
@@ -283,14 +310,15 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
 void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags) {
   if (count <= 0) return;
   TTC_REQUIRE(max_m <= QR_MAX_M, TTC_EDIM, "qr: row count exceeds the supported maximum (1536)");
-  const size_t smem = sizeof(double) * (NB * NB * 2 + NB + NW + (size_t)max_m * NB);
+  const size_t smem = sizeof(double) * (NB * NB * 2 + 3 * NB + NW + 2 + NW * 128 + (size_t)(max_m + 15) * NB);
   static int attr_dev = -1;
   static int nsm = 0;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
     TTC_CUDA(cudaFuncSetAttribute(householder_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(sizeof(double) * (NB * NB * 2 + NB + NW + (size_t)QR_MAX_M * NB))));
+                                  (int)(sizeof(double) * (NB * NB * 2 + 3 * NB + NW + 2 + NW * 128 +
+                                                          (size_t)(QR_MAX_M + 15) * NB))));
     TTC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     attr_dev = dev;
   }
