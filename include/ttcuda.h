@@ -245,6 +245,24 @@ int ttc_tt_scale(ttc_context* ctx, double a, const ttc_ttv* x, ttc_ttv_out* out)
 int ttc_rayleigh_grad(ttc_context* ctx, const ttc_tto* H, const ttc_ttv* x, int32_t ckpt_every,
                       double* value, double* const* grads);
 
+/* Householder QR of one m x n matrix in device memory that allocates nothing.
+ * No counterpart in the reference (the Julia package calls LAPACK qr on host arrays).  It
+ * is for callers that cannot allocate device memory when they need the factorisation, such
+ * as code running inside a memory pool or arena that owns the device's memory budget: its
+ * scratch (working copy of A, reflector factors, descriptor, status word) is a fixed device
+ * array of about 4.1 MiB inside the library, held by every GPU that loads it until exit.
+ * A (lda >= m), Q (m x min(m,n), ldq >= m, may be NULL) and R (min(m,n) x n upper
+ * triangular, ldr >= min(m,n), may be NULL) are device pointers on the current device; A
+ * is not modified.  Limits: m <= 1536, m*n <= 524288, min(m,n) <= 512, else TTC_EDIM and
+ * nothing runs.  Work is queued on `stream` (NULL = default stream) and the call returns
+ * without waiting.  `status` (device int32, may be NULL) is zeroed and then receives the
+ * kernel flags (2: non-finite value in A).  All calls on a device share the scratch: calls
+ * that overlap on the GPU race and must be serialised by the caller.  The first call on a
+ * device resolves the scratch address and should come before any stream capture.
+ * Errors are reported by ttc_last_error(NULL). */
+int ttc_qr_noalloc(int32_t m, int32_t n, const double* A, int64_t lda, double* Q, int64_t ldq, double* R,
+                   int64_t ldr, int32_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,6 +13,8 @@ using namespace ttc;
 namespace ttc {
 
 static thread_local std::string g_err_noctx;
+// Message of ttc_last_error(NULL) for entry points that take no context.
+void set_noctx_error(const std::string& msg) { g_err_noctx = msg; }
 
 template <class F>
 int guard(ttc_context* c, F&& f) {
