@@ -212,13 +212,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local)
     import ttcuda
+    from ttcuda import shard
 
     ctx = ttcuda.Context(local)
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
     ttcuda._CTX = ctx
 
-    dims, tts = workload(seed=7 + rank, batch=args.batch)
+    dims, tts = workload(seed=shard.rank_seed(7, rank), batch=args.batch)
     ranks = [r for _, r, _ in tts]
     tt_objs = [ttcuda.TTvector(len(d_), v, d_, r, [0] * len(d_)) for d_, r, v in tts]
     rks = heuristic(ranks)
@@ -249,12 +250,7 @@ def main():
             fn()
         e1.record(stream)
         barrier()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return shard.max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
 
     # warm-up (builds and captures the plans)
     for _ in range(max(3, args.warmup)):
@@ -274,8 +270,8 @@ def main():
     clocks = cs.summary(local)
 
     nb = len(tts) * world
-    value = nb * args.steps / (ms_mixed / 1e3)
-    fp64_value = nb * args.steps / (ms_fp64 / 1e3)
+    value = shard.whole_job_rate(len(tts), world, args.steps, ms_mixed)
+    fp64_value = shard.whole_job_rate(len(tts), world, args.steps, ms_fp64)
 
     # accuracy on the GPU: ||x - round(x)|| / ||x|| through the library (difference TT, norm)
     def rel_err(x, y):
@@ -330,22 +326,22 @@ def main():
     flops_mixed = sum(v[2] for v in prof_m.values())
     flops_fp64 = sum(v[2] for v in prof_f.values())
 
-    # end-to-end through the C ABI with host buffers (upload, round, download) every step
+    # end-to-end through the C ABI with host buffers (upload, round, download) every step; device
+    # events on the library's stream bracket the whole loop, host-side gaps included
     h2d = in_bytes
-    t0 = time.perf_counter()
     d2h = 0
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
     for _ in range(args.steps):
         xb.upload(tt_objs)
         step_mixed(sync=True)
         outs = y_mixed.download()
         d2h = sum(8 * sum(o_.ttv_dims[k] * o_.ttv_rks[k] * o_.ttv_rks[k + 1] for k in range(D)) for o_ in outs)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = nb * args.steps / e2e_s
+    e1.record(stream)
+    barrier()
+    e2e_ms = shard.max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
+    e2e_value = shard.whole_job_rate(len(tts), world, args.steps, e2e_ms)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
