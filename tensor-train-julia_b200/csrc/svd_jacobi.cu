@@ -21,9 +21,17 @@
 // the partner column of the second block moves through shared memory; the OWNT rotations
 // of a warp are independent and interleaved for instruction-level parallelism.
 //
-// Rotation (Rutishauser's formulas): with alpha = ||x||^2, beta = ||y||^2, gamma = x.y,
-// rotate when gamma^2 > tol^2 alpha beta; d = beta - alpha,
-// t = sign(d) 2 gamma / (|d| + sqrt(d^2 + 4 gamma^2)), c = 1/sqrt(1 + t^2), s = c t.
+// Rotation: with alpha = ||x||^2, beta = ||y||^2, gamma = x.y, rotate when
+// gamma^2 > tol^2 alpha beta; with d = beta - alpha and h = sqrt(d^2 + 4 gamma^2) the angle of
+// modulus <= pi/4 has cos 2theta = |d|/h, sin 2theta = sign(d) 2 gamma / h, so
+// c = sqrt((1 + cos 2theta)/2), s = sin 2theta / (2c) -- the rotation of Rutishauser's
+// t = sign(d) 2 gamma / (|d| + h), computed with two reciprocal square roots and no division.
+//
+// Inert columns: a column whose squared norm is at most the numerical-zero threshold is never
+// rotated (see make_rot), so its norm never changes.  Such columns (for example the
+// (rank-deficient) trailing columns of an oversampled randomized-rounding factor) are left
+// out of the sweeps: every CTA builds the same list of active columns and the blocks are
+// gathered from it.
 // alpha, beta, gamma are scaled by a power of two that brings ||X||_F^2 into [1/4, 1], so
 // the squares cannot overflow or underflow (the rotation is scale invariant).
 #include <cooperative_groups.h>
@@ -71,9 +79,11 @@ __device__ __forceinline__ Rot make_rot(double alpha, double beta, double gamma,
   const double g2 = gamma * gamma;
   if (!(g2 > q.tol2 * alpha * beta)) return r;
   const double d = beta - alpha;
-  const double t = copysign(1.0, d) * (2.0 * gamma) / (fabs(d) + sqrt(fma(d, d, 4.0 * g2)));
-  r.c = rsqrt(fma(t, t, 1.0));
-  r.s = r.c * t;
+  const double rh = rsqrt(fma(d, d, 4.0 * g2));
+  const double c2 = fma(0.5 * fabs(d), rh, 0.5);
+  const double rc = rsqrt(c2);
+  r.c = c2 * rc;
+  r.s = copysign(1.0, d) * gamma * rh * rc;
   r.apply = true;
   return r;
 }
@@ -220,6 +230,30 @@ __device__ __forceinline__ void copy_cols(double* __restrict__ dst, long long dl
   }
 }
 
+// One column of `rows` doubles copied by one warp (four loads in flight per lane).
+__device__ __forceinline__ void copy_col_warp(double* __restrict__ dc, const double* __restrict__ sc, int rows) {
+  const int lane = threadIdx.x & 31;
+  for (int r0 = lane; r0 < rows; r0 += 128) {
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = (r0 + 32 * u < rows) ? sc[r0 + 32 * u] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (r0 + 32 * u < rows) dc[r0 + 32 * u] = v[u];
+  }
+}
+
+// Gather the columns idx[0..cols) of a global matrix into packed shared-memory columns, or
+// scatter them back; one warp per column.
+__device__ __forceinline__ void gather_cols(double* __restrict__ dst, const double* __restrict__ src, long long ld,
+                                            const int* idx, int rows, int cols) {
+  for (int c = threadIdx.x >> 5; c < cols; c += NW) copy_col_warp(dst + (long long)c * rows, src + (long long)idx[c] * ld, rows);
+}
+__device__ __forceinline__ void scatter_cols(double* __restrict__ dst, long long ld, const double* __restrict__ src,
+                                             const int* idx, int rows, int cols) {
+  for (int c = threadIdx.x >> 5; c < cols; c += NW) copy_col_warp(dst + (long long)idx[c] * ld, src + (long long)c * rows, rows);
+}
+
 // Column position in the circle-method round robin over an even count `ne` of players.
 __device__ __forceinline__ int rr_player(int pos, int round, int ne) {
   if (pos == 0) return 0;
@@ -238,6 +272,13 @@ __device__ bool cross_dispatch(double* S0, double* S1, int m, int cI, int cJ, co
 }
 }  // namespace
 
+// Doubles of the dynamic shared memory before the active-column list: two blocks of bw
+// columns (and their W columns), at least n doubles (column norms, singular values).
+__host__ __device__ __forceinline__ size_t dyn_doubles(int bw, int m, int n, bool accw) {
+  const size_t blocks = 2 * (size_t)bw * (size_t)(m + (accw ? n : 0));
+  return blocks > (size_t)n ? blocks : (size_t)n;
+}
+
 // grid = count * csize CTAs, clusters of csize CTAs (one cluster per problem).  RMAX bounds
 // the register rows per lane of the cross phase (m <= 32 RMAX); RMAX = 8 keeps the kernel
 // within 128 registers so that two CTAs share an SM.
@@ -245,7 +286,7 @@ template <int RMAX>
 __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
     jacobi_svd_kernel(const JacobiDesc* __restrict__ descs, int bw, int csize, int* flags) {
   extern __shared__ double sm[];
-  __shared__ int s_any;
+  __shared__ int s_any, s_nact;
   __shared__ double s_red[NW];
   cg::cluster_group cluster = cg::this_cluster();
   const int crank = (int)cluster.block_rank();
@@ -254,8 +295,6 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   if (m <= 0 || n <= 0) return;                 // uniform across the cluster
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool accw = (D.W != nullptr);
-  const int nblk = (n + bw - 1) / bw;
-  const int ne = nblk + (nblk & 1);
   double* S0 = sm;
   double* S1 = sm + (size_t)bw * m;
   double* W0 = S1 + (size_t)bw * m;
@@ -268,14 +307,19 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
       D.W[(long long)j * D.ldw + i] = (i == j) ? 1.0 : 0.0;
     }
   }
-  // ||X||_F^2 (invariant under the rotations): scale and numerical-zero threshold
+  // column norms (into sm, free until the first block load) and ||X||_F^2, which the
+  // rotations leave invariant: scale and numerical-zero threshold
+  int* act = reinterpret_cast<int*>(sm + dyn_doubles(bw, m, n, accw));   // active columns
   {
     double a = 0.0;
     for (int j = warp; j < n; j += NW) {
       const double* xc = D.X + (long long)j * D.ldx;
-      for (int i = lane; i < m; i += 32) a = fma(xc[i], xc[i], a);
+      double cj = 0.0;
+      for (int i = lane; i < m; i += 32) cj = fma(xc[i], xc[i], cj);
+      cj = warp_sum(cj);
+      if (lane == 0) sm[j] = cj;
+      a += cj;
     }
-    a = warp_sum(a);
     if (lane == 0) s_red[warp] = a;
   }
   if (tid == 0) s_any = 0;
@@ -292,16 +336,31 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
     q.tol2 = tol * tol;
     q.zthr = q.tol2 * fro2 * q.sc;
   }
+  if (warp == 0) {   // the same list in every CTA of the cluster
+    int cnt = 0;
+    for (int c0 = 0; c0 < n; c0 += 32) {
+      const int c = c0 + lane;
+      const bool on = (c < n) && (sm[c] * q.sc > q.zthr);
+      const unsigned b = __ballot_sync(0xffffffffu, on);
+      if (on) act[cnt + __popc(b & ((1u << lane) - 1u))] = c;
+      cnt += __popc(b);
+    }
+    if (lane == 0) s_nact = cnt;
+  }
+  __syncthreads();
+  const int na = s_nact;
+  const int nblk = (na + bw - 1) / bw;
+  const int ne = nblk + (nblk & 1);
 
   auto load_block = [&](int blk, double* S, double* Wd) {
-    const int c0 = blk * bw, cn = min(bw, n - c0);
-    copy_cols(S, m, D.X + (long long)c0 * D.ldx, D.ldx, m, cn);
-    if (accw) copy_cols(Wd, n, D.W + (long long)c0 * D.ldw, D.ldw, n, cn);
+    const int c0 = blk * bw, cn = min(bw, na - c0);
+    gather_cols(S, D.X, D.ldx, act + c0, m, cn);
+    if (accw) gather_cols(Wd, D.W, D.ldw, act + c0, n, cn);
   };
   auto store_block = [&](int blk, const double* S, const double* Wd) {
-    const int c0 = blk * bw, cn = min(bw, n - c0);
-    copy_cols(D.X + (long long)c0 * D.ldx, D.ldx, S, m, m, cn);
-    if (accw) copy_cols(D.W + (long long)c0 * D.ldw, D.ldw, Wd, n, n, cn);
+    const int c0 = blk * bw, cn = min(bw, na - c0);
+    scatter_cols(D.X, D.ldx, S, act + c0, m, cn);
+    if (accw) scatter_cols(D.W, D.ldw, Wd, act + c0, n, cn);
   };
   cluster.sync();   // W = I visible to every CTA
 
@@ -312,7 +371,7 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
     bool any = false;
     // (a) pairs inside each block; blocks dealt to the CTAs of the cluster
     for (int blk = crank; blk < nblk; blk += csize) {
-      const int cI = min(bw, n - blk * bw);
+      const int cI = min(bw, na - blk * bw);
       load_block(blk, S0, W0);
       __syncthreads();
       const int nee = cI + (cI & 1);
@@ -334,7 +393,7 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
       for (int p = crank; p < ne / 2; p += csize) {
         const int bi = rr_player(p, rd, ne), bj = rr_player(ne - 1 - p, rd, ne);
         if (bi >= nblk || bj >= nblk) continue;
-        const int cI = min(bw, n - bi * bw), cJ = min(bw, n - bj * bw);
+        const int cI = min(bw, na - bi * bw), cJ = min(bw, na - bj * bw);
         load_block(bi, S0, W0);
         load_block(bj, S1, W1);
         __syncthreads();
@@ -391,12 +450,12 @@ int sm_count() {
 }
 }  // namespace
 
-// Block width and dynamic shared memory of a launch: two blocks of bw columns (and their W
-// columns), at least n doubles for the final singular-value pass.
+// Block width and dynamic shared memory of a launch: dyn_doubles(bw, ...) doubles and the
+// active-column list (max_n ints).
 static int jacobi_bw(int max_m, int max_n, bool accw, size_t* smem_out) {
   int bw = 16;
   auto need = [&](int b) {
-    return sizeof(double) * std::max<size_t>(2 * (size_t)b * (max_m + (accw ? max_n : 0)), (size_t)max_n);
+    return sizeof(double) * dyn_doubles(b, max_m, max_n, accw) + sizeof(int) * (size_t)max_n;
   };
   while (bw > 1 && need(bw) > 200 * 1024) bw >>= 1;
   *smem_out = need(bw);
