@@ -110,12 +110,19 @@ __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_be
     const bool cb_ok = (cb >= c_begin && cb < c_end);
     const double* colb = M + (long long)(cb_ok ? cb : c_begin) * ld + r0;
     double w00 = 0.0, w01 = 0.0, w10 = 0.0, w11 = 0.0;
-#pragma unroll 4
-    for (int k0 = 0; k0 < mp; k0 += 4) {
-      const int r = k0 + qc;
-      const double b = (cb_ok && r < mp) ? colb[r] : 0.0;
-      dmma(w00, w01, vref(V, mp_ld, jb, mp, qr, r), b);
-      dmma(w10, w11, vref(V, mp_ld, jb, mp, 8 + qr, r), b);
+    for (int k0 = 0; k0 < mp; k0 += 32) {         // 8 k-steps: all 8 loads in flight first
+      double bb[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int r = k0 + 4 * u + qc;
+        bb[u] = (cb_ok && r < mp) ? colb[r] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int r = k0 + 4 * u + qc;
+        dmma(w00, w01, vref(V, mp_ld, jb, mp, qr, r), bb[u]);
+        dmma(w10, w11, vref(V, mp_ld, jb, mp, 8 + qr, r), bb[u]);
+      }
     }
     Ws[qr * 8 + 2 * qc] = w00;
     Ws[qr * 8 + 2 * qc + 1] = w01;
@@ -143,16 +150,23 @@ __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_be
     const bool ok0 = (ca >= c_begin && ca < c_end), ok1 = (ca + 1 >= c_begin && ca + 1 < c_end);
     double* col0 = M + (long long)(ok0 ? ca : c_begin) * ld + r0;
     double* col1 = M + (long long)(ok1 ? ca + 1 : c_begin) * ld + r0;
-#pragma unroll 2
-    for (int rt = 0; rt < mp; rt += 8) {
-      const int r = rt + qr;
-      const bool rok = r < mp;
-      double d0 = (ok0 && rok) ? col0[r] : 0.0;
-      double d1 = (ok1 && rok) ? col1[r] : 0.0;
+    for (int rt0 = 0; rt0 < mp; rt0 += 32) {       // 4 row tiles: all 8 loads in flight first
+      double d0[4], d1[4];
 #pragma unroll
-      for (int sidx = 0; sidx < 4; ++sidx) dmma(d0, d1, vref(V, mp_ld, jb, mp, 4 * sidx + qc, r), ub[sidx]);
-      if (ok0 && rok) col0[r] = d0;
-      if (ok1 && rok) col1[r] = d1;
+      for (int u = 0; u < 4; ++u) {
+        const int r = rt0 + 8 * u + qr;
+        const bool rok = r < mp;
+        d0[u] = (ok0 && rok) ? col0[r] : 0.0;
+        d1[u] = (ok1 && rok) ? col1[r] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int r = rt0 + 8 * u + qr;
+#pragma unroll
+        for (int sidx = 0; sidx < 4; ++sidx) dmma(d0[u], d1[u], vref(V, mp_ld, jb, mp, 4 * sidx + qc, r), ub[sidx]);
+        if (ok0 && r < mp) col0[r] = d0[u];
+        if (ok1 && r < mp) col1[r] = d1[u];
+      }
     }
   }
 }
@@ -214,17 +228,26 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
       for (int c = jj + 1 + warp; c < jb; c += NW) {
         double* pc = P + c * mp_ld;
         const double cj = pc[jj];
-        double d = 0.0;
-        for (int r = jj + 1 + lane; r < mp; r += 32) d = fma(x[r], pc[r], d);
-        d = warp_sum(d);
+        double d = 0.0, d2 = 0.0;       // two chains
+        for (int r = jj + 1 + lane; r < mp; r += 64) {
+          d = fma(x[r], pc[r], d);
+          if (r + 32 < mp) d2 = fma(x[r + 32], pc[r + 32], d2);
+        }
+        d = warp_sum(d + d2);
         const double w = fma(scal, d, cj) * t;     // tau v^T c
         const double ws = w * scal;
-        double q = 0.0;
-        for (int r = jj + 1 + lane; r < mp; r += 32) {
+        double q = 0.0, q2 = 0.0;
+        for (int r = jj + 1 + lane; r < mp; r += 64) {
           const double u = fma(-ws, x[r], pc[r]);
           pc[r] = u;
           if (r > jj + 1) q = fma(u, u, q);
+          if (r + 32 < mp) {
+            const double u2 = fma(-ws, x[r + 32], pc[r + 32]);
+            pc[r + 32] = u2;
+            q2 = fma(u2, u2, q2);
+          }
         }
+        q += q2;
         if (c == jj + 1) {
           q = warp_sum(q);
           if (lane == 0) nrm2[(jj + 1) & 1] = q;
@@ -246,13 +269,13 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
     for (int pidx = warp; pidx < jb * jb; pidx += NW) {
       const int i = pidx / jb, l = pidx - i * jb;     // G[l][i] for l < i
       if (l < i) {
-        double g = 0.0;
-        for (int r = i + lane; r < mp; r += 32) {
+        double g = 0.0, g2 = 0.0;
+        for (int r = i + lane; r < mp; r += 64) {
           const double vi = (r == i) ? 1.0 : P[i * mp_ld + r];
-          const double vl = P[l * mp_ld + r];          // r >= i > l
-          g = fma(vl, vi, g);
+          g = fma(P[l * mp_ld + r], vi, g);              // r >= i > l
+          if (r + 32 < mp) g2 = fma(P[l * mp_ld + r + 32], P[i * mp_ld + r + 32], g2);
         }
-        g = warp_sum(g);
+        g = warp_sum(g + g2);
         if (lane == 0) G[i * NB + l] = g;
       }
     }
