@@ -187,7 +187,9 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
   double* sv = red + NW;             // NB   reflector scales 1/(alpha - beta)
   double* bet = sv + NB;             // NB   betas (diagonal of R)
   double* nrm2 = bet + NB;           // 2    squared norm below the diagonal of the next column
-  double* G = nrm2 + 2;              // NB*NB  (V^T V)
+  double* gs = nrm2 + 2;             // NB*NB  x_l . x_i below row i (l < i), unscaled
+  double* xl_i = gs + NB * NB;       // NB*NB  x_l[i] (l < i), unscaled
+  double* G = xl_i + NB * NB;        // NB*NB  (V^T V)
   double* Wscr = G + NB * NB;        // NW*128  per-warp 16 x 8 scratch of the reflector products
   double* P = Wscr + NW * 128;       // panel, (mp_ld x NB), mp_ld = 4 mod 16
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -225,7 +227,21 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
         scal = 1.0 / (alpha - beta);
       }
       const double* x = P + jj * mp_ld;
-      for (int c = jj + 1 + warp; c < jb; c += NW) {
+      // slot k of warp k mod NW: column k < jj gives x_k . x_jj below row jj (for V^T V),
+      // column k + 1 > jj gets the reflector
+      for (int k = warp; k < jb - 1; k += NW) {
+        if (k < jj) {
+          const double* pl = P + k * mp_ld;
+          double g = 0.0, g2 = 0.0;
+          for (int r = jj + 1 + lane; r < mp; r += 64) {
+            g = fma(pl[r], x[r], g);
+            if (r + 32 < mp) g2 = fma(pl[r + 32], x[r + 32], g2);
+          }
+          g = warp_sum(g + g2);
+          if (lane == 0) gs[k * NB + jj] = g;
+          continue;
+        }
+        const int c = k + 1;
         double* pc = P + c * mp_ld;
         const double cj = pc[jj];
         double d = 0.0, d2 = 0.0;       // two chains
@@ -257,6 +273,11 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
       if (tid == 0) { tau[jj] = t; sv[jj] = scal; bet[jj] = beta; }
       __syncthreads();
     }
+    for (int e = tid; e < NB * NB; e += NT) {        // unscaled x_l[i] for V^T V
+      const int i = e / NB, l = e - i * NB;
+      if (l < i && i < jb) xl_i[l * NB + i] = P[l * mp_ld + i];
+    }
+    __syncthreads();
     for (int c = warp; c < jb; c += NW) {
       double* pc = P + c * mp_ld;
       const double sc = sv[c];
@@ -264,33 +285,30 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
       if (lane == 0) pc[c] = bet[c];
     }
     __syncthreads();
-    // 3. T factor (dlarft, forward columnwise): G = V^T V by all warps, then T by one warp:
-    //    T[0:i, i] = -tau_i T[0:i, 0:i] G[0:i, i], T[i, i] = tau_i
-    for (int pidx = warp; pidx < jb * jb; pidx += NW) {
-      const int i = pidx / jb, l = pidx - i * jb;     // G[l][i] for l < i
-      if (l < i) {
-        double g = 0.0, g2 = 0.0;
-        for (int r = i + lane; r < mp; r += 64) {
-          const double vi = (r == i) ? 1.0 : P[i * mp_ld + r];
-          g = fma(P[l * mp_ld + r], vi, g);              // r >= i > l
-          if (r + 32 < mp) g2 = fma(P[l * mp_ld + r + 32], P[i * mp_ld + r + 32], g2);
-        }
-        g = warp_sum(g + g2);
-        if (lane == 0) G[i * NB + l] = g;
-      }
+    // 3. T factor.  G = V^T V (l < i) from the dot products of the panel loop:
+    //    v_l[i] = scal_l x_l[i], v_i[i] = 1, rows below i scaled by both (x unscaled there);
+    //    then T from T^{-1} + T^{-T} = V^T V (compact WY): T^{-1} = striu(G) + diag(1/tau), so
+    //    T[r][j] = -tau_r sum_{r < l <= j} G[r][l] T[l][j], T[j][j] = tau_j; lane j of warp 0
+    //    back-substitutes column j in registers (a zero tau gives a zero row, as in dlarft).
+    for (int e = tid; e < NB * NB; e += NT) {
+      const int i = e / NB, l = e - i * NB;
+      if (l < i) G[i * NB + l] = (i < jb) ? sv[l] * fma(sv[i], gs[l * NB + i], xl_i[l * NB + i]) : 0.0;
     }
     __syncthreads();
-    if (warp == 0) {
-      for (int e = lane; e < NB * NB; e += 32) T[e] = 0.0;
-      __syncwarp();
-      for (int i = 0; i < jb; ++i) {
-        double a = 0.0;
-        if (lane < i)
-          for (int l = lane; l < i; ++l) a = fma(T[l * NB + lane], G[i * NB + l], a);
-        if (lane < i) T[i * NB + lane] = -tau[i] * a;
-        if (lane == i) T[i * NB + i] = tau[i];
-        __syncwarp();
+    if (warp == 0 && lane < NB) {
+      const int j = lane;
+      double tc[NB];
+#pragma unroll
+      for (int k = 0; k < NB; ++k) tc[k] = (k == j && j < jb) ? tau[k] : 0.0;
+#pragma unroll
+      for (int r = NB - 2; r >= 0; --r) {
+        double a2 = 0.0;
+#pragma unroll
+        for (int l = r + 1; l < NB; ++l) a2 = fma(G[l * NB + r], tc[l], a2);
+        if (r < j && j < jb) tc[r] = -tau[r] * a2;
       }
+#pragma unroll
+      for (int k = 0; k < NB; ++k) T[j * NB + k] = tc[k];
     }
     __syncthreads();
     // 4. trailing update with H^T = I - V T^T V^T (this CTA's column octets)
@@ -333,14 +351,14 @@ __global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __r
 void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags) {
   if (count <= 0) return;
   TTC_REQUIRE(max_m <= QR_MAX_M, TTC_EDIM, "qr: row count exceeds the supported maximum (1536)");
-  const size_t smem = sizeof(double) * (NB * NB * 2 + 3 * NB + NW + 2 + NW * 128 + (size_t)(max_m + 15) * NB);
+  const size_t smem = sizeof(double) * (NB * NB * 4 + 3 * NB + NW + 2 + NW * 128 + (size_t)(max_m + 15) * NB);
   static int attr_dev = -1;
   static int nsm = 0;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
     TTC_CUDA(cudaFuncSetAttribute(householder_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(sizeof(double) * (NB * NB * 2 + 3 * NB + NW + 2 + NW * 128 +
+                                  (int)(sizeof(double) * (NB * NB * 4 + 3 * NB + NW + 2 + NW * 128 +
                                                           (size_t)(QR_MAX_M + 15) * NB))));
     TTC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     attr_dev = dev;
