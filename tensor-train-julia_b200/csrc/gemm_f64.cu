@@ -2,16 +2,24 @@
 // (FR*core, absorb U*S, Z = y_k W, Q^T y_k, environment updates).  One launch runs a
 // list of GemmDesc problems; CTA t finds its problem by binary search over the
 // descriptors' tile prefix sums, so ranks that differ per TT and per site share one
-// launch.  64x64x16 tiles, 256 threads, 4x4 FP64 accumulators per thread, register
-// prefetch double buffering; the C tile is staged through shared memory so that the
-// store is coalesced along whichever C stride is 1 (plain or transposed output).
+// launch.  64x64x16 tiles, 256 threads, register-prefetch double buffering of the shared
+// A/B tiles; the products run on the FP64 tensor cores (mma.sync m8n8k4), each warp owning a
+// 32 x 16 sub-tile (4 x 2 fragments of 8 x 8).  The C tile is staged through shared memory so
+// that the store is coalesced along whichever C stride is 1 (plain or transposed output).
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace ttc {
 
 namespace {
-constexpr int BM = 64, BN = 64, BK = 16, NT = 256, PAD = 65;
+// PAD = 4 mod 16 doubles: the fragment loads (4 k x 4 rows per half warp) hit distinct banks.
+constexpr int BM = 64, BN = 64, BK = 16, NT = 256, PAD = 68, PADC = 65;
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
 
 __device__ __forceinline__ int find_desc(const GemmDesc* __restrict__ d, int nd, long long tile) {
   int lo = 0, hi = nd - 1;
@@ -80,13 +88,15 @@ __global__ void __launch_bounds__(NT, 2) gemm_f64_grouped_kernel(const GemmDesc*
     }
   };
 
-  // Compute mapping: rows tx + 16*i, cols ty + 16*j (tx fastest -> conflict-free A reads).
-  const int tx = tid & 15, ty = tid >> 4;
-  double acc[4][4];
+  // Warp w owns rows wm*32 .. +31 and cols wn*16 .. +15 of the tile; fragment coordinates:
+  // A[qr][qc] = As[k + qc][i + qr], B[qc][qr] = Bs[k + qc][j + qr], D[qr][2qc + {0,1}].
+  const int warp = tid >> 5, lane = tid & 31, qr = lane >> 2, qc = lane & 3;
+  const int wm = warp & 1, wn = warp >> 1;
+  double acc[4][2][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < 2; ++j) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
 
   const int nk = ceil_div(D.k, BK);
   if (nk > 0) {
@@ -97,28 +107,31 @@ __global__ void __launch_bounds__(NT, 2) gemm_f64_grouped_kernel(const GemmDesc*
       const int cur = kt & 1;
       if (kt + 1 < nk) load_tile((kt + 1) * BK);
 #pragma unroll
-      for (int kk = 0; kk < BK; ++kk) {
-        double a[4], bv[4];
+      for (int kk = 0; kk < BK; kk += 4) {
+        double a[4], bv[2];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = As[cur][kk][tx + 16 * i];
+        for (int i = 0; i < 4; ++i) a[i] = As[cur][kk + qc][wm * 32 + 8 * i + qr];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) bv[j] = Bs[cur][kk][ty + 16 * j];
+        for (int j = 0; j < 2; ++j) bv[j] = Bs[cur][kk + qc][wn * 16 + 8 * j + qr];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bv[j], acc[i][j]);
+          for (int j = 0; j < 2; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], bv[j]);
       }
       if (kt + 1 < nk) store_tile(cur ^ 1);
       __syncthreads();
     }
   }
 
-  // Stage the C tile in shared memory (64 x 65 doubles), then store coalesced.
+  // Stage the C tile in shared memory (64 x 65 doubles, column-major), then store coalesced.
   double* Cs = smem;
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) Cs[(ty + 16 * j) * PAD + (tx + 16 * i)] = acc[i][j];
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+        Cs[(wn * 16 + 8 * j + 2 * qc + e) * PADC + (wm * 32 + 8 * i + qr)] = acc[i][j][e];
   __syncthreads();
   const bool c_colfast = (D.c_j0 == 1 && D.c_i0 != 1);
   const double alpha = D.alpha, beta = D.beta;
@@ -129,7 +142,7 @@ __global__ void __launch_bounds__(NT, 2) gemm_f64_grouped_kernel(const GemmDesc*
     if (gi < D.m && gj < D.n) {
       double* p = C + (long long)(gi % D.m0) * D.c_i0 + (long long)(gi / D.m0) * D.c_i1 +
                   (long long)(gj % D.n0) * D.c_j0 + (long long)(gj / D.n0) * D.c_j1;
-      const double v = alpha * Cs[lj * PAD + li];
+      const double v = alpha * Cs[lj * PADC + li];
       *p = (beta == 0.0) ? v : fma(beta, *p, v);
     }
   }
