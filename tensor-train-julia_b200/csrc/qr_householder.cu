@@ -1,4 +1,4 @@
-// Batched blocked Householder QR, one CTA per problem.
+// Batched blocked Householder QR, one thread-block cluster per problem.
 //
 // Replaces Julia `qr(A)` / `qr!(Z)` + `Matrix(F.Q)` (LAPACK geqrf + orgqr) on the
 // tall-skinny unfoldings of the orthogonalisation sweep (src/tt_rounding.jl:75-78) and of
@@ -110,15 +110,15 @@ __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_be
     const bool cb_ok = (cb >= c_begin && cb < c_end);
     const double* colb = M + (long long)(cb_ok ? cb : c_begin) * ld + r0;
     double w00 = 0.0, w01 = 0.0, w10 = 0.0, w11 = 0.0;
-    for (int k0 = 0; k0 < mp; k0 += 32) {         // 8 k-steps: all 8 loads in flight first
-      double bb[8];
+    for (int k0 = 0; k0 < mp; k0 += 64) {         // 16 k-steps: all 16 loads in flight first
+      double bb[16];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < 16; ++u) {
         const int r = k0 + 4 * u + qc;
         bb[u] = (cb_ok && r < mp) ? colb[r] : 0.0;
       }
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < 16; ++u) {
         const int r = k0 + 4 * u + qc;
         dmma(w00, w01, vref(V, mp_ld, jb, mp, qr, r), bb[u]);
         dmma(w10, w11, vref(V, mp_ld, jb, mp, 8 + qr, r), bb[u]);
@@ -150,17 +150,17 @@ __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_be
     const bool ok0 = (ca >= c_begin && ca < c_end), ok1 = (ca + 1 >= c_begin && ca + 1 < c_end);
     double* col0 = M + (long long)(ok0 ? ca : c_begin) * ld + r0;
     double* col1 = M + (long long)(ok1 ? ca + 1 : c_begin) * ld + r0;
-    for (int rt0 = 0; rt0 < mp; rt0 += 32) {       // 4 row tiles: all 8 loads in flight first
-      double d0[4], d1[4];
+    for (int rt0 = 0; rt0 < mp; rt0 += 64) {       // 8 row tiles: all 16 loads in flight first
+      double d0[8], d1[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
         const int r = rt0 + 8 * u + qr;
         const bool rok = r < mp;
         d0[u] = (ok0 && rok) ? col0[r] : 0.0;
         d1[u] = (ok1 && rok) ? col1[r] : 0.0;
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
         const int r = rt0 + 8 * u + qr;
 #pragma unroll
         for (int sidx = 0; sidx < 4; ++sidx) dmma(d0[u], d1[u], vref(V, mp_ld, jb, mp, 4 * sidx + qc, r), ub[sidx]);
