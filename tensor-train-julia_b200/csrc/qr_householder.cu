@@ -31,7 +31,7 @@ namespace cg = cooperative_groups;
 namespace ttc {
 namespace {
 constexpr int NB = 16;
-constexpr int NT = 256;
+constexpr int NT = 512;
 constexpr int NW = NT / 32;
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -173,7 +173,7 @@ __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_be
 }  // namespace
 
 // T layout in shared memory: T[col * NB + row] (upper triangular).
-__global__ void __launch_bounds__(NT, 2) householder_qr_kernel(const QRDesc* __restrict__ descs, int csize, int* flags) {
+__global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __restrict__ descs, int csize, int* flags) {
   extern __shared__ double sm[];
   cg::cluster_group cluster = cg::this_cluster();
   const int crank = (int)cluster.block_rank();
