@@ -118,7 +118,7 @@ __device__ bool rotate_smem(double* x, double* y, int m, double* wx, double* wy,
 // of width bw = NW * OWNT.  Warp w owns the columns a = w + NW*o of block I in registers; in
 // step s it rotates a against b = (a + s) mod bw of block J.  Requires m <= 32 * RPLT.
 template <int OWNT, int RPLT>
-__device__ __forceinline__ bool cross_regs(double* S0, double* S1, int m, int cI, int cJ, const RotCfg& q) {
+__device__ __forceinline__ bool cross_regs(double* S0, double* S1, int m, int ms, int cI, int cJ, const RotCfg& q) {
   constexpr int bw = NW * OWNT;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double xr[OWNT][RPLT];
@@ -128,7 +128,7 @@ __device__ __forceinline__ bool cross_regs(double* S0, double* S1, int m, int cI
 #pragma unroll
     for (int t = 0; t < RPLT; ++t) {
       const int r = lane + 32 * t;
-      xr[o][t] = (a < cI && r < m) ? S0[a * m + r] : 0.0;
+      xr[o][t] = (a < cI && r < m) ? S0[a * ms + r] : 0.0;
     }
   }
   bool any = false;
@@ -141,7 +141,7 @@ __device__ __forceinline__ bool cross_regs(double* S0, double* S1, int m, int cI
       const int a = warp + NW * o;
       const int b = (a + s) % bw;
       act[o] = (a < cI) && (b < cJ);
-      const double* y = S1 + b * m;
+      const double* y = S1 + b * ms;
       al[o] = 0.0; be[o] = 0.0; ga[o] = 0.0;
 #pragma unroll
       for (int t = 0; t < RPLT; ++t) {
@@ -171,7 +171,7 @@ __device__ __forceinline__ bool cross_regs(double* S0, double* S1, int m, int cI
       if (R.apply) {
         any = true;
         const int a = warp + NW * o;
-        double* y = S1 + ((a + s) % bw) * m;
+        double* y = S1 + ((a + s) % bw) * ms;
 #pragma unroll
         for (int t = 0; t < RPLT; ++t) {
           const int r = lane + 32 * t;
@@ -189,22 +189,22 @@ __device__ __forceinline__ bool cross_regs(double* S0, double* S1, int m, int cI
 #pragma unroll
     for (int t = 0; t < RPLT; ++t) {
       const int r = lane + 32 * t;
-      if (a < cI && r < m) S0[a * m + r] = xr[o][t];
+      if (a < cI && r < m) S0[a * ms + r] = xr[o][t];
     }
   }
   return any;
 }
 
 // Cross rotations through shared memory only (W accumulation, or m beyond the register path).
-__device__ bool cross_smem(double* S0, double* S1, double* W0, double* W1, int m, int n, int bw, int cI, int cJ,
-                           const RotCfg& q) {
+__device__ bool cross_smem(double* S0, double* S1, double* W0, double* W1, int m, int ms, int n, int bw, int cI,
+                           int cJ, const RotCfg& q) {
   const int warp = threadIdx.x >> 5;
   bool any = false;
   for (int s = 0; s < bw; ++s) {
     for (int a = warp; a < cI; a += NW) {
       const int b = (a + s) % bw;
       if (b < cJ)
-        any |= rotate_smem(S0 + a * m, S1 + b * m, m, W0 ? W0 + a * n : nullptr, W1 ? W1 + b * n : nullptr, n, q);
+        any |= rotate_smem(S0 + a * ms, S1 + b * ms, m, W0 ? W0 + a * n : nullptr, W1 ? W1 + b * n : nullptr, n, q);
     }
     __syncthreads();
   }
@@ -245,13 +245,71 @@ __device__ __forceinline__ void copy_col_warp(double* __restrict__ dc, const dou
 
 // Gather the columns idx[0..cols) of a global matrix into packed shared-memory columns, or
 // scatter them back; one warp per column.
-__device__ __forceinline__ void gather_cols(double* __restrict__ dst, const double* __restrict__ src, long long ld,
-                                            const int* idx, int rows, int cols) {
-  for (int c = threadIdx.x >> 5; c < cols; c += NW) copy_col_warp(dst + (long long)c * rows, src + (long long)idx[c] * ld, rows);
+__device__ __forceinline__ void gather_cols(double* __restrict__ dst, int dld, const double* __restrict__ src,
+                                            long long ld, const int* idx, int rows, int cols) {
+  for (int c = threadIdx.x >> 5; c < cols; c += NW) copy_col_warp(dst + (long long)c * dld, src + (long long)idx[c] * ld, rows);
 }
 __device__ __forceinline__ void scatter_cols(double* __restrict__ dst, long long ld, const double* __restrict__ src,
-                                             const int* idx, int rows, int cols) {
-  for (int c = threadIdx.x >> 5; c < cols; c += NW) copy_col_warp(dst + (long long)idx[c] * ld, src + (long long)c * rows, rows);
+                                             int sld, const int* idx, int rows, int cols) {
+  for (int c = threadIdx.x >> 5; c < cols; c += NW) copy_col_warp(dst + (long long)idx[c] * ld, src + (long long)c * sld, rows);
+}
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Screening of a block pair in the later sweeps: whether any column pair (a of block I, b of
+// block J; a < b inside one block) would be rotated.  The 16 x 16 Gram block S0^T S1 is formed
+// on the FP64 tensor cores (mma.sync m8n8k4; warp w: tile w mod 4, half w / 4 of the rows) and
+// tested with the column norms exactly as make_rot tests a pair.  A pair that passes needs no
+// rotation, so its blocks are left as they are.  bw == 16; every thread gets the same answer.
+__device__ bool screen_pair(const double* S0, const double* S1, int m, int ms, int cI, int cJ, bool same,
+                            const RotCfg& q, double* scr) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, qr = lane >> 2, qc = lane & 3;
+  double* nrm = scr;            // 32 column norms^2
+  double* part = scr + 32;      // 4 tiles x 64 partial sums of the upper row half
+  for (int c = warp; c < 32; c += NW) {
+    const bool ok = (c < 16) ? (c < cI) : (c - 16 < cJ);
+    const double* col = (c < 16) ? S0 + c * ms : S1 + (c - 16) * ms;
+    double a = 0.0;
+    if (ok)
+      for (int r = lane; r < m; r += 32) a = fma(col[r], col[r], a);
+    a = warp_sum(a);
+    if (lane == 0) nrm[c] = a;
+  }
+  const int t = warp & 3, ti = t >> 1, tj = t & 1, h = warp >> 2;
+  const int kh = ((m + 7) >> 3) << 2;
+  const int kbeg = h ? kh : 0, kend = h ? m : (kh < m ? kh : m);
+  const int ca = 8 * ti + qr, cb = 8 * tj + qr;
+  double ga0 = 0.0, ga1 = 0.0, gb0 = 0.0, gb1 = 0.0;   // two accumulator chains
+  for (int k0 = kbeg; k0 < kend; k0 += 8) {
+    const int k = k0 + qc, k2 = k0 + 4 + qc;
+    const double a = (k < kend && ca < cI) ? S0[ca * ms + k] : 0.0;
+    const double b = (k < kend && cb < cJ) ? S1[cb * ms + k] : 0.0;
+    const double a2 = (k2 < kend && ca < cI) ? S0[ca * ms + k2] : 0.0;
+    const double b2 = (k2 < kend && cb < cJ) ? S1[cb * ms + k2] : 0.0;
+    dmma(ga0, ga1, a, b);
+    dmma(gb0, gb1, a2, b2);
+  }
+  double g0 = ga0 + gb0, g1 = ga1 + gb1;
+  if (h == 1) { part[t * 64 + 2 * lane] = g0; part[t * 64 + 2 * lane + 1] = g1; }
+  __syncthreads();
+  int need = 0;
+  if (h == 0) {
+    g0 += part[t * 64 + 2 * lane];
+    g1 += part[t * 64 + 2 * lane + 1];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int a = 8 * ti + qr, b = 8 * tj + 2 * qc + e;
+      if (a < cI && b < cJ && (!same || a < b)) {
+        const double al = nrm[a] * q.sc, be = nrm[16 + b] * q.sc, ga = (e ? g1 : g0) * q.sc;
+        if (al > q.zthr && be > q.zthr && ga * ga > q.tol2 * al * be) need = 1;
+      }
+    }
+  }
+  return __syncthreads_or(need) != 0;
 }
 
 // Column position in the circle-method round robin over an even count `ne` of players.
@@ -263,19 +321,23 @@ __device__ __forceinline__ int rr_player(int pos, int round, int ne) {
 // Register-path dispatch on the rows per lane (bw = 16: two own columns per warp), up to
 // RMAX rows per lane.
 template <int RMAX>
-__device__ bool cross_dispatch(double* S0, double* S1, int m, int cI, int cJ, const RotCfg& q) {
+__device__ bool cross_dispatch(double* S0, double* S1, int m, int ms, int cI, int cJ, const RotCfg& q) {
   const int rpl = (m + 31) / 32;
-  if (rpl <= 2) return cross_regs<2, 2>(S0, S1, m, cI, cJ, q);
-  if (rpl <= 4) return cross_regs<2, 4>(S0, S1, m, cI, cJ, q);
-  if (RMAX <= 8 || rpl <= 8) return cross_regs<2, (RMAX < 8 ? RMAX : 8)>(S0, S1, m, cI, cJ, q);
-  return cross_regs<2, RMAX>(S0, S1, m, cI, cJ, q);
+  if (rpl <= 2) return cross_regs<2, 2>(S0, S1, m, ms, cI, cJ, q);
+  if (rpl <= 4) return cross_regs<2, 4>(S0, S1, m, ms, cI, cJ, q);
+  if (RMAX <= 8 || rpl <= 8) return cross_regs<2, (RMAX < 8 ? RMAX : 8)>(S0, S1, m, ms, cI, cJ, q);
+  return cross_regs<2, RMAX>(S0, S1, m, ms, cI, cJ, q);
 }
 }  // namespace
 
+// Column stride of the shared blocks: rows rounded up to 4 mod 16 doubles, so the tensor-core
+// fragment loads of the screening Gram (4 columns x 4 rows per half warp) hit distinct banks.
+__host__ __device__ __forceinline__ int smem_stride(int m) { return m + ((4 - m) & 15); }
+
 // Doubles of the dynamic shared memory before the active-column list: two blocks of bw
-// columns (and their W columns), at least n doubles (column norms, singular values).
-__host__ __device__ __forceinline__ size_t dyn_doubles(int bw, int m, int n, bool accw) {
-  const size_t blocks = 2 * (size_t)bw * (size_t)(m + (accw ? n : 0));
+// columns of stride ms (and their W columns), at least n doubles (column norms, singular values).
+__host__ __device__ __forceinline__ size_t dyn_doubles(int bw, int ms, int n, bool accw) {
+  const size_t blocks = 2 * (size_t)bw * (size_t)(ms + (accw ? n : 0));
   return blocks > (size_t)n ? blocks : (size_t)n;
 }
 
@@ -288,6 +350,7 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   extern __shared__ double sm[];
   __shared__ int s_any, s_nact;
   __shared__ double s_red[NW];
+  __shared__ double s_scr[32 + 4 * 64];
   cg::cluster_group cluster = cg::this_cluster();
   const int crank = (int)cluster.block_rank();
   const JacobiDesc D = descs[blockIdx.x / csize];
@@ -295,9 +358,10 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   if (m <= 0 || n <= 0) return;                 // uniform across the cluster
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool accw = (D.W != nullptr);
+  const int ms = smem_stride(m);                 // column stride of the shared blocks
   double* S0 = sm;
-  double* S1 = sm + (size_t)bw * m;
-  double* W0 = S1 + (size_t)bw * m;
+  double* S1 = sm + (size_t)bw * ms;
+  double* W0 = S1 + (size_t)bw * ms;
   double* W1 = W0 + (accw ? (size_t)bw * n : 0);
   const bool use_regs = !accw && bw == 16 && m <= 32 * RMAX;
 
@@ -309,7 +373,7 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   }
   // column norms (into sm, free until the first block load) and ||X||_F^2, which the
   // rotations leave invariant: scale and numerical-zero threshold
-  int* act = reinterpret_cast<int*>(sm + dyn_doubles(bw, m, n, accw));   // active columns
+  int* act = reinterpret_cast<int*>(sm + dyn_doubles(bw, ms, n, accw));   // active columns
   {
     double a = 0.0;
     for (int j = warp; j < n; j += NW) {
@@ -354,13 +418,13 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
 
   auto load_block = [&](int blk, double* S, double* Wd) {
     const int c0 = blk * bw, cn = min(bw, na - c0);
-    gather_cols(S, D.X, D.ldx, act + c0, m, cn);
-    if (accw) gather_cols(Wd, D.W, D.ldw, act + c0, n, cn);
+    gather_cols(S, ms, D.X, D.ldx, act + c0, m, cn);
+    if (accw) gather_cols(Wd, n, D.W, D.ldw, act + c0, n, cn);
   };
   auto store_block = [&](int blk, const double* S, const double* Wd) {
     const int c0 = blk * bw, cn = min(bw, na - c0);
-    scatter_cols(D.X, D.ldx, S, act + c0, m, cn);
-    if (accw) scatter_cols(D.W, D.ldw, Wd, act + c0, n, cn);
+    scatter_cols(D.X, D.ldx, S, ms, act + c0, m, cn);
+    if (accw) scatter_cols(D.W, D.ldw, Wd, n, act + c0, n, cn);
   };
   cluster.sync();   // W = I visible to every CTA
 
@@ -369,17 +433,19 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   int sweep = 0;
   for (; sweep < MAX_SWEEPS && !converged; ++sweep) {
     bool any = false;
+    const bool screen = (sweep >= 2) && (bw == 16);   // late sweeps: skip block pairs that need no rotation
     // (a) pairs inside each block; blocks dealt to the CTAs of the cluster
     for (int blk = crank; blk < nblk; blk += csize) {
       const int cI = min(bw, na - blk * bw);
       load_block(blk, S0, W0);
       __syncthreads();
+      if (screen && !screen_pair(S0, S0, m, ms, cI, cI, true, q, s_scr)) continue;   // block unchanged
       const int nee = cI + (cI & 1);
       for (int rd = 0; rd < nee - 1; ++rd) {
         for (int p = warp; p < nee / 2; p += NW) {
           const int i = rr_player(p, rd, nee), j = rr_player(nee - 1 - p, rd, nee);
           if (i < cI && j < cI)
-            any |= rotate_smem(S0 + i * m, S0 + j * m, m, accw ? W0 + i * n : nullptr, accw ? W0 + j * n : nullptr,
+            any |= rotate_smem(S0 + i * ms, S0 + j * ms, m, accw ? W0 + i * n : nullptr, accw ? W0 + j * n : nullptr,
                                n, q);
         }
         __syncthreads();
@@ -397,8 +463,9 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
         load_block(bi, S0, W0);
         load_block(bj, S1, W1);
         __syncthreads();
-        if (use_regs) any |= cross_dispatch<RMAX>(S0, S1, m, cI, cJ, q);
-        else any |= cross_smem(S0, S1, accw ? W0 : nullptr, accw ? W1 : nullptr, m, n, bw, cI, cJ, q);
+        if (screen && !screen_pair(S0, S1, m, ms, cI, cJ, false, q, s_scr)) continue;   // blocks unchanged
+        if (use_regs) any |= cross_dispatch<RMAX>(S0, S1, m, ms, cI, cJ, q);
+        else any |= cross_smem(S0, S1, accw ? W0 : nullptr, accw ? W1 : nullptr, m, ms, n, bw, cI, cJ, q);
         __syncthreads();
         store_block(bi, S0, W0);
         store_block(bj, S1, W1);
@@ -455,7 +522,7 @@ int sm_count() {
 static int jacobi_bw(int max_m, int max_n, bool accw, size_t* smem_out) {
   int bw = 16;
   auto need = [&](int b) {
-    return sizeof(double) * dyn_doubles(b, max_m, max_n, accw) + sizeof(int) * (size_t)max_n;
+    return sizeof(double) * dyn_doubles(b, smem_stride(max_m), max_n, accw) + sizeof(int) * (size_t)max_n;
   };
   while (bw > 1 && need(bw) > 200 * 1024) bw >>= 1;
   *smem_out = need(bw);
