@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   int sweep = 0;
   for (; sweep < MAX_SWEEPS && !converged; ++sweep) {
     bool any = false;
-    const bool screen = (sweep >= 2) && (bw == 16);   // late sweeps: skip block pairs that need no rotation
+    const bool screen = (sweep >= 3) && (bw == 16);   // late sweeps: skip block pairs that need no rotation
     // (a) pairs inside each block; blocks dealt to the CTAs of the cluster
     for (int blk = crank; blk < nblk; blk += csize) {
       const int cI = min(bw, na - blk * bw);
