@@ -35,6 +35,9 @@ sys.path.insert(0, os.path.join(ROOT, "tensor-train-julia_b200"))
 
 D, NPHYS, BATCH, RMIN, RMAX, TOL = 32, 2, 64, 16, 256, 1e-8
 METRIC = "TT roundings/s at d=32,r=256: mixed vs FP64 GPU at 1e-8 rel err; % roofline"
+# DRAM bytes (read + write) of one mixed-step Householder QR launch over 16 TTs, from
+# `ncu --set full` (profiles/householder_qr_gemm_f64_full_16tts.md): 38.0 MB + 24.1 MB.
+QR_DRAM_BYTES_16TT = 62.13e6
 
 
 # ------------------------------------------------------------------------- workload
@@ -372,7 +375,9 @@ def main():
                              "fp64_algorithmic": flops_fp64 * world * args.steps / (ms_fp64 / 1e3) / 1e9},
             "roofline": {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": fp64_peak_tflops,
                          "unit": "TFLOP/s", "frac": (achieved / fp64_peak_tflops) if achieved else None,
-                         "traffic": None,
+                         "traffic": (QR_DRAM_BYTES_16TT * len(tts) / 16.0) if dom == "householder_qr" else None,
+                         "traffic_note": "dram read+write of one mixed-step QR launch (768-row panels) in the 16-TT "
+                                         "ncu capture, scaled by TTs per launch",
                          "peak_source": "FP64 cuBLAS DGEMM 4096^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
                          "avg_launch_ms": dom_avg_ms, "launches_per_step": dom_n,
                          "profile_ms_per_step": {k: round(v[0], 3) for k, v in prof_m.items() if v[1]},
