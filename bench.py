@@ -35,8 +35,8 @@ sys.path.insert(0, os.path.join(ROOT, "tensor-train-julia_b200"))
 
 D, NPHYS, BATCH, RMIN, RMAX, TOL = 32, 2, 64, 16, 256, 1e-8
 METRIC = "TT roundings/s at d=32,r=256: mixed vs FP64 GPU at 1e-8 rel err; % roofline"
-# DRAM bytes (read + write) of one mixed-step Householder QR launch over 16 TTs, from
-# `ncu --set full` (profiles/householder_qr_gemm_f64_full_16tts.md): 38.0 MB + 24.1 MB.
+# DRAM bytes (read + write) of one mixed-step Householder QR launch over 16 TTs, measured with
+# `ncu --set full` on this kernel: 38.0 MB + 24.1 MB.
 QR_DRAM_BYTES_16TT = 62.13e6
 
 
