@@ -59,6 +59,10 @@ struct GemmDesc {
   long long c_i0, c_i1, c_j0, c_j1, c_b;
   double alpha, beta;
   long long tile_start;   // first flat tile index of this problem (prefix sum, filled by the planner)
+  // Optional device-side bound on the columns that can be nonzero (for example a truncation
+  // rank written by an earlier kernel): output columns >= *n_dev are B columns known to be zero,
+  // so their tiles store zeros (beta == 0) or are skipped (beta != 0) without the product.
+  const int* n_dev;
 };
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }

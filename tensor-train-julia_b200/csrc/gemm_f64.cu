@@ -48,6 +48,18 @@ __global__ void __launch_bounds__(NT, 2) gemm_f64_grouped_kernel(const GemmDesc*
   const int rem = (int)(local - (long long)b * per);
   const int bm = rem % tm, bn = rem / tm;
   const int row0 = bm * BM, col0 = bn * BN;
+  if (D.n_dev && col0 >= *D.n_dev) {          // every column of this tile is known to be zero
+    if (D.beta != 0.0) return;
+    double* __restrict__ Cz = D.C + (long long)b * D.c_b;
+    for (int e = threadIdx.x; e < BM * BN; e += NT) {
+      const int li = e & 63, lj = e >> 6;
+      const int gi = row0 + li, gj = col0 + lj;
+      if (gi < D.m && gj < D.n)
+        Cz[(long long)(gi % D.m0) * D.c_i0 + (long long)(gi / D.m0) * D.c_i1 + (long long)(gj % D.n0) * D.c_j0 +
+           (long long)(gj / D.n0) * D.c_j1] = 0.0;
+    }
+    return;
+  }
 
   const double* __restrict__ A = D.A + (long long)b * D.a_b;
   const double* __restrict__ B = D.B + (long long)b * D.b_b;

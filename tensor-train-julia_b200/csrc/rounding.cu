@@ -146,7 +146,9 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         tr.push_back({sig, perm, q, rank});
         sel.push_back({Rc, q, sig, perm, rank, q, q, q, Ut, q, 1});
         g1.push_back(gd(p, q, q, Q, 1, p, Ut, 1, q, y->core(t, j), yc, 1));
+        g1.back().n_dev = rank;                       // Ut is zero beyond the kept rank
         g2.push_back(gd(q, q, q, R, q, 1, Ut, 1, q, T1, 1, q));
+        g2.back().n_dev = rank;
       } else {
         // M = Q1 R1 (q > p, Q1 not formed); one-sided Jacobi on R1^T (p x p) gives V Sigma
         // in its columns: core j <- V^T (normalised columns, exactly orthonormal up to the
@@ -165,8 +167,10 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         sel.push_back({Rc, p, sig, perm, rank, p, q, p, Vt, p, 1});
         cpW.push_back(cd2(Vt, y->core(t, j), p, q, 1, p, yc, 1));
         g2.push_back(gd(q, q, p, y->core(t, j), 1, yc, Vt, 1, p, T1, 1, q));   // M V (before core j changes)
+        g2.back().n_dev = rank;                       // Vt is zero beyond the kept rank
       }
       g3.push_back(gd(ml, q, q, y->core(t, j - 1), 1, ml, T1, 1, q, T2, 1, ml));
+      g3.back().n_dev = rank;                         // T1 is zero beyond the kept rank
       cpT2.push_back(cd2(T2, y->core(t, j - 1), ml, q, 1, ml, 1, ml));
     }
     B.copy(cpX);

@@ -222,6 +222,7 @@ void check_gemm(const GemmDesc& d) {
   }
   const long long ec[5] = {mi0, mi1, ni0, ni1, d.batch}, sc[5] = {d.c_i0, d.c_i1, d.c_j0, d.c_j1, d.c_b};
   region_check(d.C, 8 * (size_t)span_elems(ec, sc, 5), "gemm C");
+  if (d.n_dev) region_check(d.n_dev, sizeof(int), "gemm n_dev");
 }
 }  // namespace
 
