@@ -381,3 +381,54 @@ def test_batched_round_rand_bf16_iid_ranks():
         assert rel(got, ref) < 1e-8
         # floor() keeps the discarded weight of each bond below tol^2 ||x||^2 (src/tt_rounding.jl:298-315)
         assert rel(got, t) < math.sqrt(len(dims) - 1) * 1e-8
+
+
+# ------------------------------------------------------------------ full configuration sizes
+def test_config2_full_size_operator_rounding_consistency():
+    """Config 2 at full size: 1D Hubbard MPO (16 sites, 32 spin-orbitals, t=1, U=4) applied to a
+    rank-128 TT, Gaussian sketch of rank 138 (block_rks=138: one block).  Rounding A y without
+    forming it (operator sketch) and forming A y first then rounding use the same sketch, so
+    they agree to FP64 rounding; <y|A|y> from the operator contraction matches dot(y, A y)."""
+    h, V = mo.hubbard_1D(16, t=1.0, U=4.0)
+    H = mo.hV_to_mpo(h, V, (2,) * 32)
+    y = o.rand_tt((2,) * 32, 128, np.random.default_rng(40), normalise=True)
+    rks = [1] + [138] * 31 + [1]
+    z_op = ttcuda.ttrand_rounding_op([1.0], op_dev(H), [to_dev(y)], rks, orthogonal=False, seed=5, block_rks=138)
+    Hy = ttcuda.mpo_apply(op_dev(H), to_dev(y))
+    assert Hy.ttv_rks == [a * b for a, b in zip(H.tto_rks, y.ttv_rks)]
+    z_apply = ttcuda.ttrand_rounding(Hy, rks, orthogonal=False, seed=5, block_rks=138)
+    assert z_op.ttv_rks == z_apply.ttv_rks
+    assert rel(z_op, z_apply) < 1e-10
+    e1 = ttcuda.dot_operator(to_dev(y), op_dev(H), to_dev(y))
+    e2 = ttcuda.dot(to_dev(y), Hy)
+    assert math.isclose(e1, e2, rel_tol=1e-10)
+
+
+def test_config4_full_size_gradient_finite_differences():
+    """Config 4 at full size: 4x4 open-boundary Hubbard lattice (t=1, U=8) in snake ordering,
+    x of rank 256, environments checkpointed every 4 sites.  The value matches
+    <x|H|x>/<x|x> from the contractions and the gradient matches central finite differences
+    (h = 1e-6) along 16 seeded random directions in core space."""
+    h, V = mo.hubbard_2D(4, 4, t=1.0, U=8.0, w_pbc=False, L_pbc=False)
+    s = mo.snake_permutation(4, 4)
+    H = op_dev(mo.hV_to_mpo(h[np.ix_(s, s)], V[np.ix_(s, s, s, s)], (2,) * 32))
+    g = np.random.default_rng(41)
+    x = o.rand_tt((2,) * 32, 256, g, normalise=True)
+    X = to_dev(x)
+    R, G = ttcuda.rayleigh_grad(H, X, ckpt_every=4)
+
+    def rq(cores):
+        t = ttcuda.TTvector(x.N, cores, x.ttv_dims, x.ttv_rks, [0] * x.N)
+        return ttcuda.dot_operator(t, H, t) / ttcuda.dot(t, t)
+
+    assert math.isclose(R, rq([c.copy() for c in x.ttv_vec]), rel_tol=1e-10)
+    hstep = 1e-6
+    for _ in range(16):
+        d = [g.standard_normal(c.shape) for c in x.ttv_vec]
+        nd = math.sqrt(sum(float(np.sum(v * v)) for v in d))
+        d = [v / nd for v in d]
+        fp = rq([np.asfortranarray(c + hstep * v) for c, v in zip(x.ttv_vec, d)])
+        fm = rq([np.asfortranarray(c - hstep * v) for c, v in zip(x.ttv_vec, d)])
+        fd = (fp - fm) / (2 * hstep)
+        an = sum(float(np.sum(np.asarray(gk).reshape(v.shape, order="F") * v)) for gk, v in zip(G, d))
+        assert abs(fd - an) <= 1e-5 * max(abs(an), 1e-3 * abs(R)), (fd, an)
