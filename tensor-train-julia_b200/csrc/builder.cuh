@@ -28,6 +28,7 @@ struct Builder {
 
   void gemm(std::vector<GemmDesc> v);
   void qr(const std::vector<QRDesc>& v);
+  void qapply(const std::vector<QApplyDesc>& v);
   void jacobi(const std::vector<JacobiDesc>& v);
   void trunc(const std::vector<TruncDesc>& v, double tol, long long rmax);
   void select(const std::vector<SelectDesc>& v);

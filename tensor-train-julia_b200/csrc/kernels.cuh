@@ -22,6 +22,18 @@ struct QRDesc {
 constexpr int QR_MAX_M = 1536;
 void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags);
 
+// B <- Q B with Q = H_1 ... H_K the Householder factor a QR launch left in A (reflectors below
+// the diagonal, T factors in Tws): B is m x nb (ld ldb); columns >= *n_dev (when given) are
+// zero and stay zero, so they are not touched.
+struct QApplyDesc {
+  int m, K;
+  const double* A; int lda;
+  const double* Tws;
+  double* B; int ldb; int nb;
+  const int* n_dev;
+};
+void launch_qr_apply(const QApplyDesc* d_descs, int count, int max_m, cudaStream_t s);
+
 // ---- batched one-sided Jacobi SVD (svd_jacobi.cu)
 // X (m x n, col-major, ldx, m >= n) is overwritten by X*W whose columns are
 // orthogonal; W (n x n, ldw) accumulates the rotations when not null.

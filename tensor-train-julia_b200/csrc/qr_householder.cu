@@ -348,6 +348,53 @@ __global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __r
   }
 }
 
+// B <- Q B from the stored panels, backwards (as the Q formation, but from B instead of the
+// identity and over all its columns).  CTA problem / csize owns the column octets o with
+// o mod csize == CTA rank; the panels are only read, so no CTA waits for another.
+__global__ void __launch_bounds__(NT, 1) householder_apply_q_kernel(const QApplyDesc* __restrict__ descs, int csize) {
+  extern __shared__ double sm[];
+  const int crank = (int)(blockIdx.x % csize);
+  const QApplyDesc D = descs[blockIdx.x / csize];
+  const int m = D.m, K = D.K;
+  if (m <= 0 || K <= 0 || D.nb <= 0) return;
+  const int nb = D.n_dev ? min(D.nb, *D.n_dev) : D.nb;
+  if (nb <= 0) return;
+  double* T = sm;                    // NB*NB
+  double* Wscr = T + NB * NB;        // NW*128
+  double* P = Wscr + NW * 128;       // panel, (mp_ld x NB)
+  const int tid = threadIdx.x;
+  const int npan = (K + NB - 1) / NB;
+  for (int p = npan - 1; p >= 0; --p) {
+    const int j0 = p * NB, jb = min(NB, K - j0), mp = m - j0, mp_ld = mp + ((4 - mp) & 15);
+    copy_cols(P, mp_ld, D.A + (long long)j0 * D.lda + j0, D.lda, mp, jb);
+    for (int e = tid; e < NB * NB; e += NT) T[e] = D.Tws[p * NB * NB + e];
+    __syncthreads();
+    apply_block_reflector(D.B, D.ldb, j0, m, 0, nb, P, mp_ld, jb, T, false, crank, csize, Wscr);
+    __syncthreads();
+  }
+}
+
+void launch_qr_apply(const QApplyDesc* d_descs, int count, int max_m, cudaStream_t s) {
+  if (count <= 0) return;
+  TTC_REQUIRE(max_m <= QR_MAX_M, TTC_EDIM, "qr apply: row count exceeds the supported maximum (1536)");
+  const size_t smem = sizeof(double) * (NB * NB + NW * 128 + (size_t)(max_m + 15) * NB);
+  static int attr_dev = -1;
+  static int nsm = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    TTC_CUDA(cudaFuncSetAttribute(householder_apply_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * (NB * NB + NW * 128 + (size_t)(QR_MAX_M + 15) * NB))));
+    TTC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    attr_dev = dev;
+  }
+  int per_sm = 1;
+  TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, householder_apply_q_kernel, NT, smem));
+  const int csize = std::min(8, std::max(1, nsm * std::max(1, per_sm) / count));
+  householder_apply_q_kernel<<<(unsigned)(count * csize), NT, smem, s>>>(d_descs, csize);
+  TTC_CHECK_LAUNCH();
+}
+
 void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags) {
   if (count <= 0) return;
   TTC_REQUIRE(max_m <= QR_MAX_M, TTC_EDIM, "qr: row count exceeds the supported maximum (1536)");

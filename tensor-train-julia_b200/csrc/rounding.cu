@@ -110,7 +110,9 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
     std::vector<JacobiDesc> jac;
     std::vector<TruncDesc> tr;
     std::vector<SelectDesc> sel;
-    std::vector<GemmDesc> g1, g2, g3;
+    std::vector<GemmDesc> g2, g3;
+    std::vector<ZeroDesc> zb;
+    std::vector<QApplyDesc> qa;
     int* infos = B.diag_ints((int)T);
     const int n = (int)y->dims[j], nl = (int)y->dims[j - 1];
     for (size_t i = 0; i < T; ++i) {
@@ -126,8 +128,8 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
       if (p >= q) {
         // M^T = Q R1 (Householder), R1^T = Q2 R2, one-sided Jacobi on R2^T = R1 Q2: same left
         // singular vectors as R1 in about half the sweeps (QR-LQ preconditioning); the factor
-        // absorbed into core j-1 stays R1^T U.
-        double* Q = B.wd((size_t)p * q);
+        // absorbed into core j-1 stays R1^T U.  Q is not formed: its stored reflectors are
+        // applied to [U; 0] (columns up to the kept rank) to give core j = (Q U)^T.
         double* R = B.wd((size_t)q * q);
         double* Y = B.wd((size_t)q * q);
         double* R2 = B.wd((size_t)q * q);
@@ -136,19 +138,20 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         int* perm = B.wi(q);
         double* Tws = B.wd(qr_tws(p, q));
         double* Tws2 = B.wd(qr_tws(q, q));
-        double* Ut = B.wd((size_t)q * q);
+        double* Bq = B.wd((size_t)p * q);           // [U; 0], then Q [U; 0]
         cpX.push_back(cd2(y->core(t, j), X, q, p, 1, yc, p, 1));
-        qr.push_back({p, q, X, p, Q, p, R, q, Tws});
+        qr.push_back({p, q, X, p, nullptr, 0, R, q, Tws});
         cpY.push_back(cd2(R, Y, q, q, 1, q, q, 1));
         qr2.push_back({q, q, Y, q, nullptr, 0, R2, q, Tws2});
         cpR.push_back(cd2(R2, Rc, q, q, 1, q, q, 1));
         jac.push_back({q, q, Rc, q, nullptr, 0, sig, perm, info});
         tr.push_back({sig, perm, q, rank});
-        sel.push_back({Rc, q, sig, perm, rank, q, q, q, Ut, q, 1});
-        g1.push_back(gd(p, q, q, Q, 1, p, Ut, 1, q, y->core(t, j), yc, 1));
-        g1.back().n_dev = rank;                       // Ut is zero beyond the kept rank
-        g2.push_back(gd(q, q, q, R, q, 1, Ut, 1, q, T1, 1, q));
-        g2.back().n_dev = rank;
+        zb.push_back({Bq, (long long)p * q});
+        sel.push_back({Rc, q, sig, perm, rank, q, q, q, Bq, p, 1});
+        g2.push_back(gd(q, q, q, R, q, 1, Bq, 1, p, T1, 1, q));
+        g2.back().n_dev = rank;                       // U is zero beyond the kept rank
+        qa.push_back({p, q, X, p, Tws, Bq, p, q, rank});
+        cpW.push_back(cd2(Bq, y->core(t, j), p, q, 1, p, yc, 1));
       } else {
         // M = Q1 R1 (q > p, Q1 not formed); one-sided Jacobi on R1^T (p x p) gives V Sigma
         // in its columns: core j <- V^T (normalised columns, exactly orthonormal up to the
@@ -180,9 +183,10 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
     B.copy(cpR);
     B.jacobi(jac);
     B.trunc(tr, tol, rmax);
+    B.zero(zb);
     B.select(sel);
-    B.gemm(g2);      // reads core j (p < q branch) before g1 / cpW overwrite it
-    B.gemm(g1);
+    B.gemm(g2);      // reads U (p >= q) or core j (p < q) before qapply / cpW overwrite them
+    B.qapply(qa);
     B.copy(cpW);
     B.gemm(g3);
     B.copy(cpT2);

@@ -79,6 +79,7 @@ static void launch_op(ttc_context* c, const Plan& p, const Op& op) {
     switch (op.kind) {
       case OP_GEMM: launch_gemm_f64((const GemmDesc*)d, op.count, op.total, s); break;
       case OP_QR: launch_qr((const QRDesc*)d, op.count, op.a, s, c->d_flags); break;
+      case OP_QAPPLY: launch_qr_apply((const QApplyDesc*)d, op.count, op.a, s); break;
       case OP_JACOBI: launch_jacobi((const JacobiDesc*)d, op.count, op.a, op.b, op.total != 0, s, c->d_flags); break;
       case OP_TRUNC: launch_truncate((const TruncDesc*)d, op.count, op.tol, op.rmax, s); break;
       case OP_SELECT: launch_select((const SelectDesc*)d, op.count, op.a, op.b, s); break;
@@ -107,6 +108,7 @@ static int op_kind(OpKind k) {
   switch (k) {
     case OP_GEMM: return TTC_KERN_GEMM_F64;
     case OP_QR: return TTC_KERN_QR;
+    case OP_QAPPLY: return TTC_KERN_QR;
     case OP_JACOBI: return TTC_KERN_JACOBI;
     case OP_BF16GEMM: return TTC_KERN_GEMM_BF16;
     case OP_APPLY: return TTC_KERN_APPLY;
@@ -289,6 +291,22 @@ void Builder::qr(const std::vector<QRDesc>& v) {
     const double m = d.m, k = std::min(d.m, d.n);
     op.flops += (d.Q ? 2.0 : 1.0) * (2.0 * m * k * k - 2.0 * k * k * k / 3.0) + 2.0 * m * k * (d.n - k);
   }
+  plan->ops.push_back(op);
+}
+void Builder::qapply(const std::vector<QApplyDesc>& v) {
+  if (v.empty()) return;
+  int mm = 0;
+  for (auto& d : v) {
+    mm = std::max(mm, d.m);
+    const bool on = wsbase != nullptr;
+    chk(on, d.A, (long long)d.lda * (d.K - 1) + d.m, 8, "qr apply A");
+    chk(on, d.Tws, (long long)((d.K + 15) / 16) * 256, 8, "qr apply Tws");
+    chk(on, d.B, (long long)d.ldb * (d.nb - 1) + d.m, 8, "qr apply B");
+    if (d.n_dev) chk(on, d.n_dev, 1, 4, "qr apply n_dev");
+    TTC_REQUIRE(d.lda >= d.m && d.ldb >= d.m && d.K <= d.m, TTC_EINTERNAL, "qr apply: leading dims");
+  }
+  Op op; op.kind = OP_QAPPLY; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm;
+  for (auto& d : v) op.flops += 4.0 * d.m * (double)d.K * d.nb - 2.0 * (double)d.K * d.K * d.nb;
   plan->ops.push_back(op);
 }
 void Builder::jacobi(const std::vector<JacobiDesc>& v) {

@@ -20,7 +20,7 @@ namespace ttc {
 
 enum OpKind {
   OP_GEMM, OP_QR, OP_JACOBI, OP_TRUNC, OP_SELECT, OP_COPY, OP_ZERO, OP_SUMSQ, OP_APPLY,
-  OP_PHILOX, OP_BF16GEMM, OP_ZEROCHK, OP_FINAL, OP_STAGE, OP_CVT_BF16, OP_SETRANK
+  OP_PHILOX, OP_BF16GEMM, OP_ZEROCHK, OP_FINAL, OP_STAGE, OP_CVT_BF16, OP_SETRANK, OP_QAPPLY
 };
 
 struct Op {
