@@ -18,6 +18,7 @@ struct QRDesc {
   double* Q; int ldq;
   double* R; int ldr;
   double* Tws;      // >= ceil(K/16)*16*16 doubles of workspace for the block reflectors
+  int r_trans;      // 1: R is written transposed, R^T[j][i] at R[i*ldr + j]
 };
 constexpr int QR_MAX_M = 1536;
 void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags);

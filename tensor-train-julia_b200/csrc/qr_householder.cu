@@ -326,8 +326,11 @@ __global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __r
   // R = upper triangle of A[0:K, 0:n]
   if (D.R) {
     for (int j = (int)(threadIdx.x >> 5) + NW * crank; j < n; j += NW * csize)
-      for (int i = (int)(threadIdx.x & 31); i < K; i += 32)
-        D.R[(long long)j * D.ldr + i] = (i <= j) ? A[(long long)j * lda + i] : 0.0;
+      for (int i = (int)(threadIdx.x & 31); i < K; i += 32) {
+        const double v = (i <= j) ? A[(long long)j * lda + i] : 0.0;
+        if (D.r_trans) D.R[(long long)i * D.ldr + j] = v;
+        else D.R[(long long)j * D.ldr + i] = v;
+      }
   }
   if (!D.Q) return;
   // Q = H_1 ... H_K [I; 0], accumulated backwards panel by panel.  Each CTA initialises

@@ -132,7 +132,6 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         // applied to [U; 0] (columns up to the kept rank) to give core j = (Q U)^T.
         double* R = B.wd((size_t)q * q);
         double* Y = B.wd((size_t)q * q);
-        double* R2 = B.wd((size_t)q * q);
         double* Rc = B.wd((size_t)q * q);
         double* sig = B.wd(q);
         int* perm = B.wi(q);
@@ -142,8 +141,7 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         cpX.push_back(cd2(y->core(t, j), X, q, p, 1, yc, p, 1));
         qr.push_back({p, q, X, p, nullptr, 0, R, q, Tws});
         cpY.push_back(cd2(R, Y, q, q, 1, q, q, 1));
-        qr2.push_back({q, q, Y, q, nullptr, 0, R2, q, Tws2});
-        cpR.push_back(cd2(R2, Rc, q, q, 1, q, q, 1));
+        qr2.push_back({q, q, Y, q, nullptr, 0, Rc, q, Tws2, 1});   // R2^T written straight into Rc
         jac.push_back({q, q, Rc, q, nullptr, 0, sig, perm, info});
         tr.push_back({sig, perm, q, rank});
         zb.push_back({Bq, (long long)p * q});
@@ -433,13 +431,16 @@ void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<i
       const double* Yk = (k == 0) ? x->core(t, 0) : Y[i];
       const long long yk_ld = (k == 0) ? (long long)x->capr(t, 0) * n : (long long)rh * n;
       double* Z = B.wd((size_t)rh * n * s);
-      double* Q = B.wd((size_t)rh * n * rhn);
+      const int yc = y->capr(t, k);
+      // Q goes straight into core k when the core's capacity equals its rank (same layout)
+      const bool direct = (yc == rh);
+      double* Q = direct ? y->core(t, k) : B.wd((size_t)rh * n * rhn);
       double* P = B.wd((size_t)rhn * r1);
       double* Tws = B.wd(qr_tws(rh * n, s));
       gz.push_back(gd(rh * n, s, r1, Yk, 1, yk_ld, W[i][k + 1], 1, r1, Z, 1, (long long)rh * n, wscale));
       qr.push_back({rh * n, s, Z, rh * n, Q, rh * n, nullptr, 0, Tws});
-      const int yc = y->capr(t, k);
-      cp.push_back(cd3(Q, y->core(t, k), rh, n, rhn, 1, rh, (long long)rh * n, 1, yc, (long long)yc * n));
+      if (!direct)
+        cp.push_back(cd3(Q, y->core(t, k), rh, n, rhn, 1, rh, (long long)rh * n, 1, yc, (long long)yc * n));
       gp.push_back(gd(rhn, r1, rh * n, Q, (long long)rh * n, 1, Yk, 1, yk_ld, P, 1, rhn));
       gy.push_back(gd(rhn, nn * r2, r1, P, 1, rhn, x->core(t, k + 1), 1, x->capr(t, k + 1), Yn[i], 1, rhn));
     }
