@@ -1,9 +1,12 @@
 // extern "C" boundary of libttcuda (declared in include/ttcuda.h).  Converts exceptions to
 // status codes, moves host tensors in the reference's column-major layout to and from the
-// internal device layout (one pinned staging copy per call, permutation on the device).
+// internal device layout (one pinned staging copy per call, packed by several host threads;
+// permutation on the device).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "api_impl.cuh"
 #include "regions.cuh"
@@ -49,6 +52,35 @@ void ensure_stage(ttc_context* c, size_t bytes) {
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Host copies of a transfer (dst, src, bytes), split over host threads: packing hundreds of MB
+// into the pinned staging buffer is bound by host memory bandwidth, which one thread does not
+// reach.  Small transfers stay on the calling thread.
+struct HostCopy { void* dst; const void* src; size_t bytes; };
+static void parallel_memcpy(const std::vector<HostCopy>& cps) {
+  size_t total = 0;
+  for (const auto& c : cps) total += c.bytes;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nt = (unsigned)std::min<size_t>(std::min(hw, 16u), total / (8u << 20) + 1);
+  if (nt <= 1) {
+    for (const auto& c : cps) std::memcpy(c.dst, c.src, c.bytes);
+    return;
+  }
+  // split the byte range [0, total) evenly; a copy may be cut between two threads
+  auto work = [&](size_t lo, size_t hi) {
+    size_t base = 0;
+    for (const auto& c : cps) {
+      const size_t a = std::max(lo, base), e = std::min(hi, base + c.bytes);
+      if (a < e) std::memcpy((char*)c.dst + (a - base), (const char*)c.src + (a - base), e - a);
+      base += c.bytes;
+      if (base >= hi) break;
+    }
+  };
+  std::vector<std::thread> th;
+  for (unsigned i = 1; i < nt; ++i) th.emplace_back(work, total * i / nt, total * (i + 1) / nt);
+  work(0, total / nt);
+  for (auto& t : th) t.join();
+}
+
 void validate_ttv(const ttc_ttv* x) {
   TTC_REQUIRE(x && x->N > 0 && x->dims && x->rks && x->cores, TTC_EARG, "TTvector: null field");
   for (int k = 0; k < x->N; ++k) {
@@ -86,6 +118,7 @@ void batch_upload_many(ttc_batch* b, int first, int m, const ttc_ttv* xs, bool r
   int* hr = (int*)(h + off_rk);
   size_t o = 0, ci = 0;
   long long maxe = 0;
+  std::vector<HostCopy> hcp;
   for (int i = 0; i < m; ++i) {
     const ttc_ttv& x = xs[i];
     const int t = first + i;
@@ -93,7 +126,7 @@ void batch_upload_many(ttc_batch* b, int first, int m, const ttc_ttv* xs, bool r
       const int kx = reverse ? N - 1 - k : k;     // host core feeding slot core k
       const long long n = x.dims[kx], r0 = x.rks[kx], r1 = x.rks[kx + 1], cap0 = b->capr(t, k);
       const size_t cnt = (size_t)n * r0 * r1;
-      std::memcpy(hd + o, x.cores[kx], cnt * sizeof(double));
+      hcp.push_back({hd + o, x.cores[kx], cnt * sizeof(double)});
       // Julia (i, a, b) at i + n*(a + r0*b)  ->  internal (a, i, b) at a + cap0*(i + n*b);
       // reversed: internal (b, i, a) at b + cap0*(i + n*a)
       if (!reverse)
@@ -105,6 +138,7 @@ void batch_upload_many(ttc_batch* b, int first, int m, const ttc_ttv* xs, bool r
     }
     for (int k = 0; k <= N; ++k) hr[(size_t)i * (N + 1) + k] = (int)x.rks[reverse ? N - k : k];
   }
+  parallel_memcpy(hcp);
   // zero the slots (padding must be 0), then copy data + descriptors + ranks in one transfer
   TTC_CUDA(cudaMemsetAsync(b->core(first, 0), 0, sizeof(double) * (b->tt_off[first + m] - b->tt_off[first]), c->stream));
   TTC_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, c->stream));
@@ -170,13 +204,18 @@ void batch_download_many(ttc_batch* b, int first, int m, ttc_ttv_out* ys, bool r
   TTC_CUDA(cudaMemcpyAsync(h, d, data * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   TTC_CUDA(cudaStreamSynchronize(c->stream));
   size_t q = 0;
+  std::vector<HostCopy> hcp;
   for (int i = 0; i < m; ++i) {
     const int t = first + i;
     for (int ko = 0; ko < N; ++ko) {
       const int k = reverse ? N - 1 - ko : ko;
       const size_t cnt = (size_t)b->dims[k] * b->rk(t, k) * b->rk(t, k + 1);
-      std::memcpy(ys[i].cores[ko], (double*)h + offs[q++], cnt * sizeof(double));
+      hcp.push_back({ys[i].cores[ko], (double*)h + offs[q++], cnt * sizeof(double)});
     }
+  }
+  parallel_memcpy(hcp);
+  for (int i = 0; i < m; ++i) {
+    const int t = first + i;
     for (int k = 0; k <= N; ++k) ys[i].rks[k] = b->rk(t, reverse ? N - k : k);
     if (ys[i].ot)
       for (int k = 0; k < N; ++k)
