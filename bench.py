@@ -339,7 +339,7 @@ def main():
     for _ in range(args.steps):
         xb.upload(tt_objs)
         step_mixed(sync=True)
-        outs = y_mixed.download()
+        outs = y_mixed.download(reuse=True)
         d2h = sum(8 * sum(o_.ttv_dims[k] * o_.ttv_rks[k] * o_.ttv_rks[k + 1] for k in range(D)) for o_ in outs)
     e1.record(stream)
     barrier()
@@ -385,7 +385,8 @@ def main():
             "kernel_profile_fp64_ms": {k: round(v[0], 3) for k, v in prof_f.items() if v[1]},
             "jacobi_sweeps": {"mixed": sw_m, "fp64": sw_f},
             "e2e": {"value": e2e_value, "unit": "roundings/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+                    "d2h_bytes_per_step": int(d2h),
+                    "path": "DeviceBatch.upload (host numpy cores) -> round_rand -> download into reused host buffers"},
             "gpu_launches": int(launches_m * args.steps + launches_f * args.steps),
             "clocks": clocks,
         }

@@ -533,8 +533,16 @@ class DeviceBatch:
         self.ctx.check(lib.ttc_batch_ranks(self.h, int(i), r.ctypes.data_as(L.P_i64)))
         return [int(v) for v in r]
 
-    def download(self) -> List[TTvector]:
-        outs = [_Out(self.dims, c) for c in self.caps]
+    def download(self, reuse: bool = False) -> List[TTvector]:
+        """The batch's TTs as host TTvectors.  With reuse=True the host buffers of the previous
+        reusing download are written again (no allocation; the TTvectors it returned then see
+        the new values), as a loop that rounds and downloads the same basis repeatedly wants."""
+        if reuse:
+            outs = getattr(self, "_outs", None)
+            if outs is None:
+                outs = self._outs = [_Out(self.dims, c) for c in self.caps]
+        else:
+            outs = [_Out(self.dims, c) for c in self.caps]
         arr = (L.TTVOut * len(outs))(*[o.s for o in outs])
         self.ctx.check(lib.ttc_batch_download_all(self.h, arr))
         # the library wrote ranks, ot and cores through the pointers each _Out holds

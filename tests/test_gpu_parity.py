@@ -432,3 +432,22 @@ def test_config4_full_size_gradient_finite_differences():
         fd = (fp - fm) / (2 * hstep)
         an = sum(float(np.sum(np.asarray(gk).reshape(v.shape, order="F") * v)) for gk, v in zip(G, d))
         assert abs(fd - an) <= 1e-5 * max(abs(an), 1e-3 * abs(R)), (fd, an)
+
+
+def test_batch_download_reuse_matches_fresh_buffers():
+    """DeviceBatch.download(reuse=True) writes into the same host buffers on every call and
+    returns what a fresh download returns."""
+    dims = (2,) * 10
+    tts = [decaying_tt(dims, o.r_and_d_to_rks([1] + [10] * 9 + [1], dims), seed=500 + i, decay_per=3.0)
+           for i in range(3)]
+    xb = ttcuda.DeviceBatch.from_tts([to_dev(t) for t in tts])
+    yb = ttcuda.DeviceBatch(dims, [t.ttv_rks for t in tts])
+    xb.round_det(yb, tol=1e-4)
+    fresh = yb.download()
+    a = yb.download(reuse=True)
+    b = yb.download(reuse=True)
+    for f, u, v in zip(fresh, a, b):
+        assert f.ttv_rks == u.ttv_rks == v.ttv_rks
+        for c1, c2, c3 in zip(f.ttv_vec, u.ttv_vec, v.ttv_vec):
+            assert np.array_equal(c1, c2) and np.array_equal(c2, c3)
+            assert np.shares_memory(c2, c3)
