@@ -264,8 +264,8 @@ def main():
     # L2: the resident inputs (sum of core bytes) exceed the 126 MB L2
     in_bytes = sum(8 * sum(d_[k] * r[k] * r[k + 1] for k in range(D)) for d_, r, _ in tts)
 
-    clock_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
-    os.makedirs(os.path.dirname(clock_path), exist_ok=True)
+    import tempfile
+    clock_path = os.path.join(tempfile.gettempdir(), f"ttc_bench_clocks_rank{rank}_{os.getpid()}.csv")
     with ClockSampler(clock_path) as cs:
         ms_mixed = timed(step_mixed, args.steps)
         ms_fp64 = timed(step_fp64, args.steps)
