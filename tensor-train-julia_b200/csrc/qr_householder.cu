@@ -109,21 +109,39 @@ __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_be
     const int cb = c0 + qr;
     const bool cb_ok = (cb >= c_begin && cb < c_end);
     const double* colb = M + (long long)(cb_ok ? cb : c_begin) * ld + r0;
-    double w00 = 0.0, w01 = 0.0, w10 = 0.0, w11 = 0.0;
-    for (int k0 = 0; k0 < mp; k0 += 64) {         // 16 k-steps: all 16 loads in flight first
-      double bb[16];
+    // 32-row chunks, the next chunk's loads in flight while the current one is multiplied;
+    // even and odd k-steps accumulate into separate tiles (four independent MMA chains)
+    double w00 = 0.0, w01 = 0.0, w10 = 0.0, w11 = 0.0, x00 = 0.0, x01 = 0.0, x10 = 0.0, x11 = 0.0;
+    double ba[8], bn[8];
+    auto load8 = [&](double (&bb)[8], int k0) {
 #pragma unroll
-      for (int u = 0; u < 16; ++u) {
+      for (int u = 0; u < 8; ++u) {
         const int r = k0 + 4 * u + qc;
         bb[u] = (cb_ok && r < mp) ? colb[r] : 0.0;
       }
+    };
+    auto mma8 = [&](const double (&bb)[8], int k0) {
 #pragma unroll
-      for (int u = 0; u < 16; ++u) {
+      for (int u = 0; u < 8; u += 2) {
         const int r = k0 + 4 * u + qc;
         dmma(w00, w01, vref(V, mp_ld, jb, mp, qr, r), bb[u]);
         dmma(w10, w11, vref(V, mp_ld, jb, mp, 8 + qr, r), bb[u]);
+        dmma(x00, x01, vref(V, mp_ld, jb, mp, qr, r + 4), bb[u + 1]);
+        dmma(x10, x11, vref(V, mp_ld, jb, mp, 8 + qr, r + 4), bb[u + 1]);
       }
+    };
+    load8(ba, 0);
+    for (int k0 = 0;; k0 += 64) {
+      const bool more1 = k0 + 32 < mp;
+      if (more1) load8(bn, k0 + 32);
+      mma8(ba, k0);
+      if (!more1) break;
+      const bool more2 = k0 + 64 < mp;
+      if (more2) load8(ba, k0 + 64);
+      mma8(bn, k0 + 32);
+      if (!more2) break;
     }
+    w00 += x00; w01 += x01; w10 += x10; w11 += x11;
     Ws[qr * 8 + 2 * qc] = w00;
     Ws[qr * 8 + 2 * qc + 1] = w01;
     Ws[(8 + qr) * 8 + 2 * qc] = w10;
@@ -150,29 +168,119 @@ __device__ void apply_block_reflector(double* M, int ld, int r0, int m, int c_be
     const bool ok0 = (ca >= c_begin && ca < c_end), ok1 = (ca + 1 >= c_begin && ca + 1 < c_end);
     double* col0 = M + (long long)(ok0 ? ca : c_begin) * ld + r0;
     double* col1 = M + (long long)(ok1 ? ca + 1 : c_begin) * ld + r0;
-    for (int rt0 = 0; rt0 < mp; rt0 += 64) {       // 8 row tiles: all 16 loads in flight first
-      double d0[8], d1[8];
+    // 32-row sets of four 8-row tiles, the next set's loads in flight while the current one is
+    // multiplied and stored
+    double da0[4], da1[4], dn0[4], dn1[4];
+    auto load4 = [&](double (&d0)[4], double (&d1)[4], int rt0) {
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < 4; ++u) {
         const int r = rt0 + 8 * u + qr;
         const bool rok = r < mp;
         d0[u] = (ok0 && rok) ? col0[r] : 0.0;
         d1[u] = (ok1 && rok) ? col1[r] : 0.0;
       }
+    };
+    auto upd4 = [&](double (&d0)[4], double (&d1)[4], int rt0) {
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < 4; ++u) {
         const int r = rt0 + 8 * u + qr;
 #pragma unroll
         for (int sidx = 0; sidx < 4; ++sidx) dmma(d0[u], d1[u], vref(V, mp_ld, jb, mp, 4 * sidx + qc, r), ub[sidx]);
         if (ok0 && r < mp) col0[r] = d0[u];
         if (ok1 && r < mp) col1[r] = d1[u];
       }
+    };
+    load4(da0, da1, 0);
+    for (int rt0 = 0;; rt0 += 64) {
+      const bool more1 = rt0 + 32 < mp;
+      if (more1) load4(dn0, dn1, rt0 + 32);
+      upd4(da0, da1, rt0);
+      if (!more1) break;
+      const bool more2 = rt0 + 64 < mp;
+      if (more2) load4(da0, da1, rt0 + 64);
+      upd4(dn0, dn1, rt0 + 32);
+      if (!more2) break;
     }
   }
 }
 }  // namespace
 
+// Column steps of a panel held in registers (panel rows mp <= 32 * RMAX): warp w keeps panel
+// column (w + 1) mod NW, lane l its rows l + 32 i, for the whole panel.  Step jj reads only the
+// reflector column x = P[:, jj] and its diagonal from shared memory: the warps of the columns
+// c > jj apply reflector jj to their column (x unscaled, as in the shared-memory loop below),
+// the warps of the finished columns c < jj form x_c . x_jj below row jj for V^T V, and the warp
+// of column jj + 1 returns its squared norm below the diagonal and publishes the column to P,
+// where it is the next step's reflector.  Every column reaches P at the step that finishes it.
+template <int RMAX>
+__device__ __forceinline__ void panel_steps_regs(double* P, int mp, int mp_ld, int jb, double* nrm2, double* tau,
+                                                 double* sv, double* bet, double* gs) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int c = (warp + 1) % NW;
+  const bool own = c < jb;
+  double* pc = P + c * mp_ld;
+  double cr[RMAX];
+#pragma unroll
+  for (int i = 0; i < RMAX; ++i) {
+    const int r = lane + 32 * i;
+    cr[i] = (own && r < mp) ? pc[r] : 0.0;
+  }
+  for (int jj = 0; jj < jb; ++jj) {
+    const double s = nrm2[jj & 1];
+    const double alpha = P[jj * mp_ld + jj];
+    double beta, t, scal;
+    if (s == 0.0) { t = 0.0; beta = alpha; scal = 0.0; }
+    else {
+      beta = -copysign(sqrt(fma(alpha, alpha, s)), alpha);
+      t = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    const double* x = P + jj * mp_ld;
+    if (own && c != jj) {
+      double dd[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int i = 0; i < RMAX; ++i) {
+        const int r = lane + 32 * i;
+        const double xv = (r > jj && r < mp) ? x[r] : 0.0;
+        dd[i & 3] = fma(xv, cr[i], dd[i & 3]);
+      }
+      const double d = warp_sum((dd[0] + dd[1]) + (dd[2] + dd[3]));
+      if (c < jj) {
+        if (lane == 0) gs[c * NB + jj] = d;
+      } else {
+        const double cj = __shfl_sync(0xffffffffu, cr[0], jj);   // row jj < 32: lane jj, i = 0
+        const double w = fma(scal, d, cj) * t;                   // tau v^T c
+        const double ws = w * scal;
+        double qq[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < RMAX; ++i) {
+          const int r = lane + 32 * i;
+          if (r > jj && r < mp) {
+            cr[i] = fma(-ws, x[r], cr[i]);
+            if (r > jj + 1) qq[i & 3] = fma(cr[i], cr[i], qq[i & 3]);
+          }
+        }
+        if (lane == jj) cr[0] = cj - w;
+        if (c == jj + 1) {
+          const double q = warp_sum((qq[0] + qq[1]) + (qq[2] + qq[3]));
+          if (lane == 0) nrm2[(jj + 1) & 1] = q;
+#pragma unroll
+          for (int i = 0; i < RMAX; ++i) {
+            const int r = lane + 32 * i;
+            if (r < mp) pc[r] = cr[i];
+          }
+        }
+      }
+    }
+    if (tid == 0) { tau[jj] = t; sv[jj] = scal; bet[jj] = beta; }
+    __syncthreads();
+  }
+}
+
 // T layout in shared memory: T[col * NB + row] (upper triangular).
+// RMAX > 0: panels of at most 32 * RMAX rows factored from registers (panel_steps_regs);
+// RMAX = 0: the shared-memory column loop.
+template <int RMAX>
 __global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __restrict__ descs, int csize, int* flags) {
   extern __shared__ double sm[];
   cg::cluster_group cluster = cg::this_cluster();
@@ -216,7 +324,8 @@ __global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __r
       if (tid == 0) nrm2[0] = s0;
       __syncthreads();
     }
-    for (int jj = 0; jj < jb; ++jj) {
+    if constexpr (RMAX > 0) panel_steps_regs<RMAX>(P, mp, mp_ld, jb, nrm2, tau, sv, bet, gs);
+    else for (int jj = 0; jj < jb; ++jj) {
       const double s = nrm2[jj & 1];
       const double alpha = P[jj * mp_ld + jj];
       double beta, t, scal;
@@ -398,24 +507,27 @@ void launch_qr_apply(const QApplyDesc* d_descs, int count, int max_m, cudaStream
   TTC_CHECK_LAUNCH();
 }
 
-void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags) {
-  if (count <= 0) return;
-  TTC_REQUIRE(max_m <= QR_MAX_M, TTC_EDIM, "qr: row count exceeds the supported maximum (1536)");
-  const size_t smem = sizeof(double) * (NB * NB * 4 + 3 * NB + NW + 2 + NW * 128 + (size_t)(max_m + 15) * NB);
+namespace {
+size_t qr_smem(int max_m) {
+  return sizeof(double) * (NB * NB * 4 + 3 * NB + NW + 2 + NW * 128 + (size_t)(max_m + 15) * NB);
+}
+
+template <int RMAX>
+void launch_qr_cfg(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags) {
+  const size_t smem = qr_smem(max_m);
   static int attr_dev = -1;
   static int nsm = 0;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
-    TTC_CUDA(cudaFuncSetAttribute(householder_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(sizeof(double) * (NB * NB * 4 + 3 * NB + NW + 2 + NW * 128 +
-                                                          (size_t)(QR_MAX_M + 15) * NB))));
+    TTC_CUDA(cudaFuncSetAttribute(householder_qr_kernel<RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)qr_smem(RMAX > 0 ? 32 * RMAX : QR_MAX_M)));
     TTC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     attr_dev = dev;
   }
   // CTAs per problem: fill the resident-CTA slots of the GPU, at most 8 (portable cluster)
   int per_sm = 1;
-  TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, householder_qr_kernel, NT, smem));
+  TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, householder_qr_kernel<RMAX>, NT, smem));
   const int slots = nsm * std::max(1, per_sm);
   int c = std::min(8, std::max(1, slots / count));
   int csize = 1;
@@ -432,8 +544,19 @@ void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int*
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  TTC_CUDA(cudaLaunchKernelEx(&cfg, householder_qr_kernel, d_descs, csize, d_flags));
+  TTC_CUDA(cudaLaunchKernelEx(&cfg, householder_qr_kernel<RMAX>, d_descs, csize, d_flags));
   TTC_CHECK_LAUNCH();
+}
+}  // namespace
+
+void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags) {
+  if (count <= 0) return;
+  TTC_REQUIRE(max_m <= QR_MAX_M, TTC_EDIM, "qr: row count exceeds the supported maximum (1536)");
+  // Register panels up to 512 rows; at 768 rows (24 rows per lane) the column and the loads in
+  // flight no longer fit the 128 registers of a 512-thread CTA and the shared-memory loop wins.
+  if (max_m <= 256) launch_qr_cfg<8>(d_descs, count, max_m, s, d_flags);
+  else if (max_m <= 512) launch_qr_cfg<16>(d_descs, count, max_m, s, d_flags);
+  else launch_qr_cfg<0>(d_descs, count, max_m, s, d_flags);
 }
 
 }  // namespace ttc

@@ -84,7 +84,8 @@ def test_gemm_transposed_and_split(ctx):
     assert np.allclose(got, ref, rtol=1e-13, atol=1e-12)
 
 
-@pytest.mark.parametrize("m,n", [(1, 1), (7, 3), (3, 7), (64, 64), (100, 37), (512, 256), (300, 300), (1044, 522)])
+@pytest.mark.parametrize("m,n", [(1, 1), (7, 3), (3, 7), (64, 64), (100, 37), (512, 256), (300, 300), (768, 384),
+                                 (700, 690), (1044, 522)])
 def test_householder_qr(ctx, m, n):
     g = np.random.default_rng(m + n)
     A = g.standard_normal((m, n))
