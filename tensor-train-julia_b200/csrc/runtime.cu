@@ -1,4 +1,6 @@
 // Plan execution, small control kernels, context and batch management of libttcuda.
+#include <cstdio>
+#include <cstdlib>
 #include <algorithm>
 #include <cmath>
 #include <cuda_bf16.h>
@@ -144,13 +146,21 @@ static void run_plan_profiled(ttc_context* c, Plan& p) {
   }
   TTC_CUDA(cudaStreamSynchronize(c->stream));
   for (int k = 0; k < 8; ++k) { c->stats.kind_ms[k] = 0; c->stats.kind_launches[k] = 0; c->stats.kind_flops[k] = 0; }
-  for (size_t j = 0; j < kinds.size(); ++j) {
+  // TTC_PROFILE_TRACE=<file>: one line per launch appended (op kind, problems, the kernel-specific
+  // size arguments a, b and total, device ms, algorithmic FLOPs)
+  FILE* trace = getenv("TTC_PROFILE_TRACE") ? fopen(getenv("TTC_PROFILE_TRACE"), "a") : nullptr;
+  size_t j = 0;
+  for (const Op& op : p.ops) {
+    if (op.kind == OP_STAGE) continue;
     float ms = 0;
     TTC_CUDA(cudaEventElapsedTime(&ms, ev[2 * j], ev[2 * j + 1]));
     c->stats.kind_ms[kinds[j]] += ms;
     c->stats.kind_launches[kinds[j]] += 1;
     c->stats.kind_flops[kinds[j]] += flops[j];
+    if (trace) fprintf(trace, "%d %d %d %d %lld %.4f %.4g\n", (int)op.kind, op.count, op.a, op.b, op.total, ms, flops[j]);
+    ++j;
   }
+  if (trace) fclose(trace);
   for (auto e : ev) cudaEventDestroy(e);
   // Jacobi sweep counters written into the plan blob
   c->stats.jacobi_problems = 0; c->stats.jacobi_sweeps_sum = 0; c->stats.jacobi_sweeps_max = 0;
@@ -274,9 +284,10 @@ void Builder::gemm(std::vector<GemmDesc> v) {
 }
 void Builder::qr(const std::vector<QRDesc>& v) {
   if (v.empty()) return;
-  int mm = 0;
+  int mm = 0, nn = 0;
   for (auto& d : v) {
     mm = std::max(mm, d.m);
+    nn = std::max(nn, d.n);
     const int K = std::min(d.m, d.n);
     const bool on = wsbase != nullptr;
     chk(on, d.A, (long long)d.lda * (d.n - 1) + d.m, 8, "qr A");
@@ -287,7 +298,7 @@ void Builder::qr(const std::vector<QRDesc>& v) {
     TTC_REQUIRE(d.lda >= d.m && (!d.Q || d.ldq >= d.m) && (!d.R || d.ldr >= (d.r_trans ? d.n : K)), TTC_EINTERNAL,
                 "qr: leading dims");
   }
-  Op op; op.kind = OP_QR; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm;
+  Op op; op.kind = OP_QR; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm; op.b = nn;
   for (auto& d : v) {
     const double m = d.m, k = std::min(d.m, d.n);
     op.flops += (d.Q ? 2.0 : 1.0) * (2.0 * m * k * k - 2.0 * k * k * k / 3.0) + 2.0 * m * k * (d.n - k);

@@ -16,24 +16,68 @@ __device__ __forceinline__ double warp_sum(double v) {
 }  // namespace
 
 // ---------------------------------------------------------------- strided copy
-__global__ void copy4_kernel(const CopyDesc* __restrict__ descs) {
+// A 2-D copy that is contiguous along dim 0 on one side and along dim 1 on the other (a
+// transpose) goes through 32 x 32 shared-memory tiles so both the loads and the stores are
+// coalesced; every other copy maps consecutive threads to consecutive dim-0 elements, with
+// 32-bit index arithmetic when the copy has fewer than 2^31 elements.
+__global__ void __launch_bounds__(NT) copy4_kernel(const CopyDesc* __restrict__ descs) {
+  __shared__ double tile[32][33];
   const CopyDesc D = descs[blockIdx.y];
-  const long long e0 = D.ext[0], e1 = D.ext[1], e2 = D.ext[2], e3 = D.ext[3];
+  long long e0 = D.ext[0], e1 = D.ext[1];
+  const long long e2 = D.ext[2], e3 = D.ext[3];
+  long long s0 = D.ss[0], s1 = D.ss[1], d0 = D.ds[0], d1 = D.ds[1];
+  if (e2 == 1 && e3 == 1 && s1 == 1 && d0 == 1 && s0 != 1) {   // orient: source contiguous along dim 0
+    long long t = e0; e0 = e1; e1 = t;
+    t = s0; s0 = s1; s1 = t;
+    t = d0; d0 = d1; d1 = t;
+  }
+  if (e2 == 1 && e3 == 1 && s0 == 1 && d1 == 1 && d0 != 1 && e0 >= 32 && e1 >= 32) {
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;     // 32 x 8 threads
+    const long long t0 = (e0 + 31) / 32, ntile = t0 * ((e1 + 31) / 32);
+    for (long long ti = blockIdx.x; ti < ntile; ti += gridDim.x) {
+      const long long b0 = (ti % t0) * 32, b1 = (ti / t0) * 32;
+#pragma unroll
+      for (int k = 0; k < 32; k += NT / 32) {
+        const long long i0 = b0 + tx, i1 = b1 + ty + k;
+        if (i0 < e0 && i1 < e1) tile[ty + k][tx] = D.src[i0 + i1 * s1];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < 32; k += NT / 32) {
+        const long long i0 = b0 + ty + k, i1 = b1 + tx;
+        if (i0 < e0 && i1 < e1) D.dst[i0 * d0 + i1] = D.alpha * tile[tx][ty + k];
+      }
+      __syncthreads();
+    }
+    return;
+  }
   const long long total = e0 * e1 * e2 * e3;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
+  if (total < (1LL << 31)) {
+    const unsigned u0 = (unsigned)e0, u1 = (unsigned)e1, u2 = (unsigned)e2;
+    for (unsigned e = blockIdx.x * NT + threadIdx.x; e < (unsigned)total; e += gridDim.x * NT) {
+      unsigned r = e;
+      const unsigned i0 = r % u0; r /= u0;
+      const unsigned i1 = r % u1; r /= u1;
+      const unsigned i2 = r % u2, i3 = r / u2;
+      const double v = D.src[i0 * s0 + i1 * s1 + i2 * D.ss[2] + i3 * D.ss[3]];
+      D.dst[i0 * d0 + i1 * d1 + i2 * D.ds[2] + i3 * D.ds[3]] = D.alpha * v;
+    }
+    return;
+  }
+  for (long long e = (long long)blockIdx.x * NT + threadIdx.x; e < total; e += (long long)gridDim.x * NT) {
     long long r = e;
     const long long i0 = r % e0; r /= e0;
     const long long i1 = r % e1; r /= e1;
     const long long i2 = r % e2; const long long i3 = r / e2;
-    const double v = D.src[i0 * D.ss[0] + i1 * D.ss[1] + i2 * D.ss[2] + i3 * D.ss[3]];
-    D.dst[i0 * D.ds[0] + i1 * D.ds[1] + i2 * D.ds[2] + i3 * D.ds[3]] = D.alpha * v;
+    const double v = D.src[i0 * s0 + i1 * s1 + i2 * D.ss[2] + i3 * D.ss[3]];
+    D.dst[i0 * d0 + i1 * d1 + i2 * D.ds[2] + i3 * D.ds[3]] = D.alpha * v;
   }
 }
 
 void launch_copy(const CopyDesc* d, int count, long long max_elems, cudaStream_t s) {
   if (count <= 0 || max_elems <= 0) return;
-  const long long blocks = std::min<long long>((max_elems + NT - 1) / NT, 148LL * 8);
+  // about four elements per thread; with `count` copies in the grid's y dimension
+  const long long blocks = std::min<long long>((max_elems + 4 * NT - 1) / (4 * NT), 148LL * 8);
   dim3 grid((unsigned)blocks, (unsigned)count);
   copy4_kernel<<<grid, NT, 0, s>>>(d);
   TTC_CHECK_LAUNCH();
