@@ -8,6 +8,13 @@ namespace ttc {
 void launch_gemm_f64(const GemmDesc* d_descs, int nd, long long total_tiles, cudaStream_t s);
 long long gemm_tiles(const GemmDesc& d);
 
+// Device-side size bound: min(cap, mult * *p) when p is given (a rank that an earlier kernel of
+// the same plan wrote), else cap.  Rows or columns beyond the bound are exactly zero in the
+// operand, so the kernels leave them out.
+__device__ __forceinline__ int dev_bound(int cap, const int* p, int mult) {
+  return p ? min(cap, max(0, mult * *p)) : cap;
+}
+
 // ---- batched Householder QR (qr_householder.cu)
 // A (m x n, col-major, lda) is overwritten.  Q (m x K, ldq) and R (K x n, ldr),
 // K = min(m, n), like LAPACK geqrf + orgqr (Julia `qr`, `Matrix(F.Q)`, `F.R`).
@@ -19,6 +26,10 @@ struct QRDesc {
   double* R; int ldr;
   double* Tws;      // >= ceil(K/16)*16*16 doubles of workspace for the block reflectors
   int r_trans;      // 1: R is written transposed, R^T[j][i] at R[i*ldr + j]
+  // optional device bounds: rows >= m_mult * *m_dev and columns >= n_mult * *n_dev of A are
+  // zero; the factorization runs on the bounded block (Q and R keep their full shapes)
+  const int* m_dev; int m_mult;
+  const int* n_dev; int n_mult;
 };
 constexpr int QR_MAX_M = 1536;
 void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags);
@@ -32,6 +43,7 @@ struct QApplyDesc {
   const double* Tws;
   double* B; int ldb; int nb;
   const int* n_dev;
+  const int* m_dev; int m_mult;   // the row bound the QR launch was given (Q acts on those rows)
 };
 void launch_qr_apply(const QApplyDesc* d_descs, int count, int max_m, cudaStream_t s);
 
@@ -46,6 +58,7 @@ struct JacobiDesc {
   double* sigma;    // n
   int* perm;        // n
   int* info;        // optional: sweeps used (negative if the sweep cap was hit)
+  const int* m_dev; int m_mult;   // optional: rows >= m_mult * *m_dev of X are zero
 };
 void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, bool accw, cudaStream_t s,
                    int* d_flags);

@@ -286,9 +286,11 @@ __global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __r
   cg::cluster_group cluster = cg::this_cluster();
   const int crank = (int)cluster.block_rank();
   const QRDesc D = descs[blockIdx.x / csize];
-  const int m = D.m, n = D.n;
-  if (m <= 0 || n <= 0) return;
-  const int K = min(m, n);
+  if (D.m <= 0 || D.n <= 0) return;
+  // the factored block (rows and columns beyond the device bounds are zero) and the shapes of
+  // R (Kc x D.n) and Q (D.m x Kc)
+  const int m = dev_bound(D.m, D.m_dev, D.m_mult), n = dev_bound(D.n, D.n_dev, D.n_mult);
+  const int K = min(m, n), Kc = min(D.m, D.n);
   double* T = sm;                    // NB*NB
   double* tau = T + NB * NB;         // NB
   double* red = tau + NB;            // NW
@@ -432,10 +434,10 @@ __global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __r
   }
   if (nonfinite && crank == 0 && threadIdx.x == 0) atomicOr(flags, DFLAG_NONFINITE);
 
-  // R = upper triangle of A[0:K, 0:n]
+  // R = upper triangle of A[0:Kc, 0:D.n] (zero outside the factored block)
   if (D.R) {
-    for (int j = (int)(threadIdx.x >> 5) + NW * crank; j < n; j += NW * csize)
-      for (int i = (int)(threadIdx.x & 31); i < K; i += 32) {
+    for (int j = (int)(threadIdx.x >> 5) + NW * crank; j < D.n; j += NW * csize)
+      for (int i = (int)(threadIdx.x & 31); i < Kc; i += 32) {
         const double v = (i <= j) ? A[(long long)j * lda + i] : 0.0;
         if (D.r_trans) D.R[(long long)i * D.ldr + j] = v;
         else D.R[(long long)j * D.ldr + i] = v;
@@ -444,18 +446,21 @@ __global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __r
   if (!D.Q) return;
   // Q = H_1 ... H_K [I; 0], accumulated backwards panel by panel.  Each CTA initialises
   // and updates only its own column octets, so the panels need no barrier between them.
-  for (int c = 0; c < K; ++c) {
+  // The reflectors act on rows < m; identity columns c >= K are untouched unless a column
+  // bound leaves some of them with c < m.
+  for (int c = 0; c < Kc; ++c) {
     if (((c >> 3) % csize) != crank) continue;
-    for (int i = tid; i < m; i += NT) D.Q[(long long)c * D.ldq + i] = (i == c) ? 1.0 : 0.0;
+    for (int i = tid; i < D.m; i += NT) D.Q[(long long)c * D.ldq + i] = (i == c) ? 1.0 : 0.0;
   }
   __syncthreads();
+  const int qc_end = (n < D.n) ? Kc : K;
   const int npan = (K + NB - 1) / NB;
   for (int p = npan - 1; p >= 0; --p) {
     const int j0 = p * NB, jb = min(NB, K - j0), mp = m - j0, mp_ld = mp + ((4 - mp) & 15);
     copy_cols(P, mp_ld, A + (long long)j0 * lda + j0, lda, mp, jb);
     for (int e = tid; e < NB * NB; e += NT) T[e] = D.Tws[p * NB * NB + e];
     __syncthreads();
-    apply_block_reflector(D.Q, D.ldq, j0, m, j0, K, P, mp_ld, jb, T, false, crank, csize, Wscr);
+    apply_block_reflector(D.Q, D.ldq, j0, m, j0, qc_end, P, mp_ld, jb, T, false, crank, csize, Wscr);
     __syncthreads();
   }
 }
@@ -467,7 +472,7 @@ __global__ void __launch_bounds__(NT, 1) householder_apply_q_kernel(const QApply
   extern __shared__ double sm[];
   const int crank = (int)(blockIdx.x % csize);
   const QApplyDesc D = descs[blockIdx.x / csize];
-  const int m = D.m, K = D.K;
+  const int m = dev_bound(D.m, D.m_dev, D.m_mult), K = min(D.K, m);   // H_k = I for k >= m
   if (m <= 0 || K <= 0 || D.nb <= 0) return;
   const int nb = D.n_dev ? min(D.nb, *D.n_dev) : D.nb;
   if (nb <= 0) return;

@@ -121,6 +121,10 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
       const int yc = y->capr(t, j), ycl = y->capr(t, j - 1);
       const int ml = ycl * nl;
       int* rank = y->drk(t, j);
+      // core j is zero beyond the kept rank r' of bond j+1 (truncated at step j+1, or the
+      // boundary rank 1), so its unfolding has n r' nonzero (n, r_{j+1}) combinations, the last
+      // ones in the device layout: the factorizations below run on that block
+      const int* rk1 = y->drk(t, j + 1);
       int* info = infos + i;
       double* X = B.wd((size_t)p * q);
       double* T1 = B.wd((size_t)q * q);
@@ -139,16 +143,17 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         double* Tws2 = B.wd(qr_tws(q, q));
         double* Bq = B.wd((size_t)p * q);           // [U; 0], then Q [U; 0]
         cpX.push_back(cd2(y->core(t, j), X, q, p, 1, yc, p, 1));
-        qr.push_back({p, q, X, p, nullptr, 0, R, q, Tws});
+        qr.push_back({p, q, X, p, nullptr, 0, R, q, Tws, 0, rk1, n, nullptr, 0});
         cpY.push_back(cd2(R, Y, q, q, 1, q, q, 1));
-        qr2.push_back({q, q, Y, q, nullptr, 0, Rc, q, Tws2, 1});   // R2^T written straight into Rc
-        jac.push_back({q, q, Rc, q, nullptr, 0, sig, perm, info});
+        // R1 has rows >= n r' zero, so R1^T has those columns zero and R2^T those rows
+        qr2.push_back({q, q, Y, q, nullptr, 0, Rc, q, Tws2, 1, nullptr, 0, rk1, n});   // R2^T into Rc
+        jac.push_back({q, q, Rc, q, nullptr, 0, sig, perm, info, rk1, n});
         tr.push_back({sig, perm, q, rank});
         zb.push_back({Bq, (long long)p * q});
         sel.push_back({Rc, q, sig, perm, rank, q, q, q, Bq, p, 1});
         g2.push_back(gd(q, q, q, R, q, 1, Bq, 1, p, T1, 1, q));
         g2.back().n_dev = rank;                       // U is zero beyond the kept rank
-        qa.push_back({p, q, X, p, Tws, Bq, p, q, rank});
+        qa.push_back({p, q, X, p, Tws, Bq, p, q, rank, rk1, n});
         cpW.push_back(cd2(Bq, y->core(t, j), p, q, 1, p, yc, 1));
       } else {
         // M = Q1 R1 (q > p, Q1 not formed); one-sided Jacobi on R1^T (p x p) gives V Sigma
@@ -161,9 +166,9 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         double* Tws = B.wd(qr_tws(q, p));
         double* Vt = B.wd((size_t)p * q);
         cpX.push_back(cd2(y->core(t, j), X, q, p, 1, yc, 1, q));
-        qr.push_back({q, p, X, q, nullptr, 0, R, p, Tws});
+        qr.push_back({q, p, X, q, nullptr, 0, R, p, Tws, 0, nullptr, 0, rk1, n});   // columns >= n r' zero
         cpR.push_back(cd2(R, Rc, p, p, p, 1, 1, p));          // Rc = R1^T
-        jac.push_back({p, p, Rc, p, nullptr, 0, sig, perm, info});
+        jac.push_back({p, p, Rc, p, nullptr, 0, sig, perm, info, rk1, n});   // rows >= n r' zero
         tr.push_back({sig, perm, p, rank});
         sel.push_back({Rc, p, sig, perm, rank, p, q, p, Vt, p, 1});
         cpW.push_back(cd2(Vt, y->core(t, j), p, q, 1, p, yc, 1));

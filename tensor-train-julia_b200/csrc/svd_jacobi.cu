@@ -354,8 +354,10 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   cg::cluster_group cluster = cg::this_cluster();
   const int crank = (int)cluster.block_rank();
   const JacobiDesc D = descs[blockIdx.x / csize];
-  const int m = D.m, n = D.n;
-  if (m <= 0 || n <= 0) return;                 // uniform across the cluster
+  if (D.m <= 0 || D.n <= 0) return;             // uniform across the cluster
+  // rows beyond the device bound are zero and stay zero under the rotations (at least one row
+  // is kept so that an all-zero problem still reports its zero singular values)
+  const int m = max(1, dev_bound(D.m, D.m_dev, D.m_mult)), n = D.n;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool accw = (D.W != nullptr);
   const int ms = smem_stride(m);                 // column stride of the shared blocks
@@ -393,7 +395,7 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   for (int i = 0; i < NW; ++i) fro2 += s_red[i];
   RotCfg q;
   {
-    const double tol = jac_tol(m);
+    const double tol = jac_tol(D.m);   // the stored row count, whatever the device bound
     int e2 = 0;
     if (fro2 > 0.0 && isfinite(fro2)) { frexp(fro2, &e2); e2 = (e2 + 1) & ~1; }   // even exponent
     q.sc = (fro2 > 0.0 && isfinite(fro2)) ? ldexp(1.0, -e2) : 1.0;
