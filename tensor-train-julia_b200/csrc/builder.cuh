@@ -62,5 +62,10 @@ ttc_batch* batch_create(ttc_context* c, int count, int N, const long long* dims,
 void batch_destroy(ttc_batch* b);
 void batch_sync_ranks(ttc_batch* b);
 std::string batch_key(const ttc_batch* b);
+// Key of a batch that a plan only writes (zeroed and given its ranks by the plan itself): its
+// identity, whatever its current rank state.
+std::string batch_out_key(const ttc_batch* b);
+// version = hash of the host ranks and orthogonality flags (after an upload or a rank sync).
+void batch_rehash(ttc_batch* b);
 
 }  // namespace ttc

@@ -56,6 +56,10 @@ static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // into the pinned staging buffer is bound by host memory bandwidth, which one thread does not
 // reach.  Small transfers stay on the calling thread.
 struct HostCopy { void* dst; const void* src; size_t bytes; };
+// Host staging is done in chunks of about this many bytes, each chunk's transfer overlapping
+// the staging of the next.
+constexpr size_t kStageChunk = 48u << 20;
+
 static void parallel_memcpy(const std::vector<HostCopy>& cps) {
   size_t total = 0;
   for (const auto& c : cps) total += c.bytes;
@@ -138,16 +142,24 @@ void batch_upload_many(ttc_batch* b, int first, int m, const ttc_ttv* xs, bool r
     }
     for (int k = 0; k <= N; ++k) hr[(size_t)i * (N + 1) + k] = (int)x.rks[reverse ? N - k : k];
   }
-  parallel_memcpy(hcp);
-  // zero the slots (padding must be 0), then copy data + descriptors + ranks in one transfer
+  // zero the slots (padding must be 0); stage the cores chunk by chunk, each chunk's transfer
+  // running while the next one is staged; then the descriptors and ranks
   TTC_CUDA(cudaMemsetAsync(b->core(first, 0), 0, sizeof(double) * (b->tt_off[first + m] - b->tt_off[first]), c->stream));
-  TTC_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, c->stream));
+  size_t sent = 0;
+  for (size_t gi = 0; gi < hcp.size();) {
+    size_t gj = gi, bytes = 0;
+    while (gj < hcp.size() && (gj == gi || bytes < kStageChunk)) bytes += hcp[gj++].bytes;
+    parallel_memcpy(std::vector<HostCopy>(hcp.begin() + (long)gi, hcp.begin() + (long)gj));
+    TTC_CUDA(cudaMemcpyAsync(d + sent, h + sent, bytes, cudaMemcpyHostToDevice, c->stream));
+    sent += bytes;
+    gi = gj;
+  }
+  TTC_CUDA(cudaMemcpyAsync(d + off_desc, h + off_desc, total - off_desc, cudaMemcpyHostToDevice, c->stream));
   launch_copy((const CopyDesc*)(d + off_desc), (int)ci, maxe, c->stream);
   TTC_CUDA(cudaMemcpyAsync(b->drk(first, 0), d + off_rk, (size_t)m * (N + 1) * sizeof(int), cudaMemcpyDeviceToDevice,
                            c->stream));
   TTC_CUDA(cudaMemsetAsync(b->d_zero + first, 0, sizeof(int) * m, c->stream));
   TTC_CUDA(cudaStreamSynchronize(c->stream));   // the pinned staging is reused by the next call
-  unsigned long long hsh = 1469598103934665603ull;
   for (int i = 0; i < m; ++i) {
     const ttc_ttv& x = xs[i];
     const int t = first + i;
@@ -155,9 +167,7 @@ void batch_upload_many(ttc_batch* b, int first, int m, const ttc_ttv* xs, bool r
     for (int k = 0; k < N; ++k)
       b->h_ot[(size_t)t * N + k] = x.ot ? (reverse ? -(int)x.ot[N - 1 - k] : (int)x.ot[k]) : 0;
   }
-  for (int v : b->h_rks) hsh = (hsh ^ (unsigned)v) * 1099511628211ull;
-  for (int v : b->h_ot) hsh = (hsh ^ (unsigned)(v + 7)) * 1099511628211ull;
-  b->version = hsh;
+  batch_rehash(b);
   b->rks_dirty = false;
 }
 
@@ -201,8 +211,6 @@ void batch_download_many(ttc_batch* b, int first, int m, ttc_ttv_out* ys, bool r
   }
   TTC_CUDA(cudaMemcpyAsync(d + off_desc, h + off_desc, nd * sizeof(CopyDesc), cudaMemcpyHostToDevice, c->stream));
   launch_copy((const CopyDesc*)(d + off_desc), (int)ci, maxe, c->stream);
-  TTC_CUDA(cudaMemcpyAsync(h, d, data * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  TTC_CUDA(cudaStreamSynchronize(c->stream));
   size_t q = 0;
   std::vector<HostCopy> hcp;
   for (int i = 0; i < m; ++i) {
@@ -213,7 +221,34 @@ void batch_download_many(ttc_batch* b, int first, int m, ttc_ttv_out* ys, bool r
       hcp.push_back({ys[i].cores[ko], (double*)h + offs[q++], cnt * sizeof(double)});
     }
   }
-  parallel_memcpy(hcp);
+  // transfer chunk by chunk, an event after each; unpack a chunk while the next ones arrive
+  std::vector<std::pair<size_t, size_t>> groups;   // [gi, gj) of hcp
+  std::vector<cudaEvent_t> evs;
+  size_t sent = 0;
+  try {
+    for (size_t gi = 0; gi < hcp.size();) {
+      size_t gj = gi, bytes = 0;
+      while (gj < hcp.size() && (gj == gi || bytes < kStageChunk)) bytes += hcp[gj++].bytes;
+      cudaEvent_t e;
+      TTC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      evs.push_back(e);
+      TTC_CUDA(cudaMemcpyAsync(h + sent, d + sent, bytes, cudaMemcpyDeviceToHost, c->stream));
+      TTC_CUDA(cudaEventRecord(e, c->stream));
+      groups.push_back({gi, gj});
+      sent += bytes;
+      gi = gj;
+    }
+    for (size_t g = 0; g < groups.size(); ++g) {
+      TTC_CUDA(cudaEventSynchronize(evs[g]));
+      parallel_memcpy(std::vector<HostCopy>(hcp.begin() + (long)groups[g].first, hcp.begin() + (long)groups[g].second));
+    }
+  } catch (...) {
+    cudaStreamSynchronize(c->stream);
+    for (auto e : evs) cudaEventDestroy(e);
+    throw;
+  }
+  TTC_CUDA(cudaStreamSynchronize(c->stream));
+  for (auto e : evs) cudaEventDestroy(e);
   for (int i = 0; i < m; ++i) {
     const int t = first + i;
     for (int k = 0; k <= N; ++k) ys[i].rks[k] = b->rk(t, reverse ? N - k : k);
@@ -252,10 +287,20 @@ ttc_batch* batch_empty_like(ttc_context* c, int count, int N, const std::vector<
 
 void record_stats(ttc_context* c, int nstages) {
   TTC_CUDA(cudaStreamSynchronize(c->stream));
+  // an event pair that cannot be timed reports 0 (its error is consumed here, so that it is
+  // not picked up by a later launch check)
+  auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
+    float v = 0.0f;
+    if (cudaEventElapsedTime(&v, a, b) != cudaSuccess) {
+      cudaGetLastError();
+      v = 0.0f;
+    }
+    return v;
+  };
   float ms[8] = {0};
-  for (int i = 0; i + 1 < nstages; ++i) cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]);
-  float tot = 0;
-  cudaEventElapsedTime(&tot, c->ev[0], c->ev[nstages - 1]);
+  if (!c->last_run_graph)   // stage events are recorded only outside CUDA graphs
+    for (int i = 0; i + 1 < nstages; ++i) ms[i] = elapsed(c->ev[i], c->ev[i + 1]);
+  const float tot = elapsed(c->ev[kEvRunBegin], c->ev[kEvRunEnd]);
   c->stats.total_ms = tot;
   c->stats.sketch_ms = 0; c->stats.orth_ms = 0; c->stats.svd_ms = 0;
   if (nstages == 3) { c->stats.orth_ms = ms[0]; c->stats.svd_ms = ms[1]; }

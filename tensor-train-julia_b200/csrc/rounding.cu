@@ -264,7 +264,7 @@ void round_det(ttc_context* c, ttc_batch* x, const ttc_round_opts& o, ttc_batch*
   }
   char kb[128];
   snprintf(kb, sizeof kb, "det:%.17g:%lld:", o.tol, (long long)o.rmax);
-  const std::string key = std::string(kb) + batch_key(x) + batch_key(y);
+  const std::string key = std::string(kb) + batch_key(x) + batch_out_key(y);
   Plan* p = get_plan(c, key, [&](Builder& B) {
     B.stage(0);
     emit_zero_tts(B, y, all);
@@ -504,7 +504,7 @@ void round_rand(ttc_context* c, ttc_batch* x, const std::vector<long long>& rks,
   char kb[256];
   snprintf(kb, sizeof kb, "rand:%d:%llu:%lld:%d:%d:%.17g:%lld:", o.orthogonal, (unsigned long long)o.seed,
            (long long)o.block_rks, o.precision, after ? 1 : 0, after ? after->tol : 0.0, after ? (long long)after->rmax : 0LL);
-  std::string key = std::string(kb) + raw_key + batch_key(x) + batch_key(y);
+  std::string key = std::string(kb) + raw_key + batch_key(x) + batch_out_key(y);
   for (long long r : rks) key += std::to_string(r) + ",";
   Plan* p = get_plan(c, key, [&](Builder& B) {
     B.stage(0);

@@ -70,8 +70,11 @@ Plan::~Plan() {
 
 static void launch_op(ttc_context* c, const Plan& p, const Op& op);
 
-static void launch_ops(ttc_context* c, Plan& p) {
-  for (const Op& op : p.ops) launch_op(c, p, op);
+// stages = false leaves the stage events out (graph capture: the whole run is timed by the
+// begin/end events around the graph launch instead)
+static void launch_ops(ttc_context* c, Plan& p, bool stages) {
+  for (const Op& op : p.ops)
+    if (stages || op.kind != OP_STAGE) launch_op(c, p, op);
 }
 
 static void launch_op(ttc_context* c, const Plan& p, const Op& op) {
@@ -179,12 +182,17 @@ static void run_plan_profiled(ttc_context* c, Plan& p) {
 
 void run_plan(ttc_context* c, Plan& p) {
   c->stats.kernel_launches = count_launches(p);
+  c->last_run_graph = false;
+  TTC_CUDA(cudaEventRecord(c->ev[kEvRunBegin], c->stream));
   if (c->profiling) {
     run_plan_profiled(c, p);
+    TTC_CUDA(cudaEventRecord(c->ev[kEvRunEnd], c->stream));
     return;
   }
   if (p.gexec && p.graph_stream == c->stream) {
     TTC_CUDA(cudaGraphLaunch(p.gexec, c->stream));
+    c->last_run_graph = true;
+    TTC_CUDA(cudaEventRecord(c->ev[kEvRunEnd], c->stream));
     return;
   }
   if (c->use_graphs && p.launches > 0) {
@@ -192,7 +200,7 @@ void run_plan(ttc_context* c, Plan& p) {
     cudaGraph_t g = nullptr;
     TTC_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     try {
-      launch_ops(c, p);
+      launch_ops(c, p, false);
     } catch (...) {
       cudaStreamEndCapture(c->stream, &g);
       if (g) cudaGraphDestroy(g);
@@ -207,10 +215,13 @@ void run_plan(ttc_context* c, Plan& p) {
     p.gexec = ge;
     p.graph_stream = c->stream;
     TTC_CUDA(cudaGraphLaunch(p.gexec, c->stream));
+    c->last_run_graph = true;
+    TTC_CUDA(cudaEventRecord(c->ev[kEvRunEnd], c->stream));
     return;
   }
-  launch_ops(c, p);
+  launch_ops(c, p, true);
   p.launches++;
+  TTC_CUDA(cudaEventRecord(c->ev[kEvRunEnd], c->stream));
 }
 
 // ---------------------------------------------------------------- builder
@@ -635,6 +646,7 @@ void batch_sync_ranks(ttc_batch* b) {
     if (z[t])
       for (int k = 0; k < b->N; ++k) b->h_ot[(size_t)t * b->N + k] = 0;
   b->rks_dirty = false;
+  batch_rehash(b);   // plans that read the batch are keyed on its rank state, not on its history
 }
 
 void batch_destroy(ttc_batch* b) {
@@ -654,6 +666,17 @@ void batch_destroy(ttc_batch* b) {
 
 std::string batch_key(const ttc_batch* b) {
   return "@" + std::to_string((unsigned long long)(uintptr_t)b) + ":" + std::to_string(b->version) + ";";
+}
+
+std::string batch_out_key(const ttc_batch* b) {
+  return "@" + std::to_string((unsigned long long)(uintptr_t)b) + ":out;";
+}
+
+void batch_rehash(ttc_batch* b) {
+  unsigned long long h = 1469598103934665603ull;   // FNV-1a over the host rank and ot state
+  for (int v : b->h_rks) h = (h ^ (unsigned)v) * 1099511628211ull;
+  for (int v : b->h_ot) h = (h ^ (unsigned)(v + 7)) * 1099511628211ull;
+  b->version = h;
 }
 
 }  // namespace ttc

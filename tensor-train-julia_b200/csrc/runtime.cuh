@@ -17,6 +17,8 @@
 #include "kernels.cuh"
 
 namespace ttc {
+// context events 6 and 7 bracket every plan run (its total device time)
+constexpr int kEvRunBegin = 6, kEvRunEnd = 7;
 
 enum OpKind {
   OP_GEMM, OP_QR, OP_JACOBI, OP_TRUNC, OP_SELECT, OP_COPY, OP_ZERO, OP_SUMSQ, OP_APPLY,
@@ -85,7 +87,8 @@ struct ttc_context {
   char* ws = nullptr;
   size_t ws_bytes = 0;
   ttc_stats stats{};
-  cudaEvent_t ev[8]{};
+  cudaEvent_t ev[8]{};              // stage events 0..3 of a plan run; kEvRunBegin/kEvRunEnd
+  bool last_run_graph = false;      // the last plan ran as a CUDA graph (no stage events)
   std::unordered_map<std::string, std::unique_ptr<ttc::Plan>> plans;
   bool use_graphs = true;
   void* d_stage = nullptr;          // device staging for uploads/downloads
