@@ -297,11 +297,16 @@ def main():
         return {"problems": st["jacobi_problems"], "mean": round(st["jacobi_sweeps_sum"] / n_, 2),
                 "max": st["jacobi_sweeps_max"]}
 
+    # NVTX ranges name the profiled steps for ncu (--nvtx --nvtx-include "ttc_mixed_step/")
+    torch.cuda.nvtx.range_push("ttc_mixed_step")
     step_mixed(sync=True)
+    torch.cuda.nvtx.range_pop()
     prof_m = ctx.kernel_profile()
     st = ctx.stats()
     launches_m, sw_m = st["kernel_launches"], sweeps(st)
+    torch.cuda.nvtx.range_push("ttc_fp64_step")
     step_fp64(sync=True)
+    torch.cuda.nvtx.range_pop()
     prof_f = ctx.kernel_profile()
     st = ctx.stats()
     launches_f, sw_f = st["kernel_launches"], sweeps(st)

@@ -123,6 +123,9 @@ typedef struct {
   double kind_flops[8];
   /* one-sided Jacobi SVDs of the last profiled call: problems, total and largest sweep count */
   int64_t jacobi_problems, jacobi_sweeps_sum, jacobi_sweeps_max;
+  /* execution plans built since the context was created (a repeated call with the same
+   * shapes reuses its plan and replays it as a CUDA graph) */
+  int64_t plans_built;
 } ttc_stats;
 
 /* Per-kernel-family timing of subsequent calls (0 = off, the default). */

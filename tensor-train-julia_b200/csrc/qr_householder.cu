@@ -278,9 +278,6 @@ __device__ __forceinline__ void panel_steps_regs(double* P, int mp, int mp_ld, i
 }
 
 // T layout in shared memory: T[col * NB + row] (upper triangular).
-// RMAX > 0: panels of at most 32 * RMAX rows factored from registers (panel_steps_regs);
-// RMAX = 0: the shared-memory column loop.
-template <int RMAX>
 __global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __restrict__ descs, int csize, int* flags) {
   extern __shared__ double sm[];
   cg::cluster_group cluster = cg::this_cluster();
@@ -326,7 +323,11 @@ __global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __r
       if (tid == 0) nrm2[0] = s0;
       __syncthreads();
     }
-    if constexpr (RMAX > 0) panel_steps_regs<RMAX>(P, mp, mp_ld, jb, nrm2, tau, sv, bet, gs);
+    // the panel's own row count picks the column-step routine (uniform across the cluster):
+    // registers up to 512 rows, else the shared-memory loop below (the register column and the
+    // loads in flight no longer fit 128 registers at 24 rows per lane)
+    if (mp <= 256) panel_steps_regs<8>(P, mp, mp_ld, jb, nrm2, tau, sv, bet, gs);
+    else if (mp <= 512) panel_steps_regs<16>(P, mp, mp_ld, jb, nrm2, tau, sv, bet, gs);
     else for (int jj = 0; jj < jb; ++jj) {
       const double s = nrm2[jj & 1];
       const double alpha = P[jj * mp_ld + jj];
@@ -517,7 +518,6 @@ size_t qr_smem(int max_m) {
   return sizeof(double) * (NB * NB * 4 + 3 * NB + NW + 2 + NW * 128 + (size_t)(max_m + 15) * NB);
 }
 
-template <int RMAX>
 void launch_qr_cfg(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags) {
   const size_t smem = qr_smem(max_m);
   static int attr_dev = -1;
@@ -525,14 +525,14 @@ void launch_qr_cfg(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, 
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
-    TTC_CUDA(cudaFuncSetAttribute(householder_qr_kernel<RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)qr_smem(RMAX > 0 ? 32 * RMAX : QR_MAX_M)));
+    TTC_CUDA(cudaFuncSetAttribute(householder_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)qr_smem(QR_MAX_M)));
     TTC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     attr_dev = dev;
   }
   // CTAs per problem: fill the resident-CTA slots of the GPU, at most 8 (portable cluster)
   int per_sm = 1;
-  TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, householder_qr_kernel<RMAX>, NT, smem));
+  TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, householder_qr_kernel, NT, smem));
   const int slots = nsm * std::max(1, per_sm);
   int c = std::min(8, std::max(1, slots / count));
   int csize = 1;
@@ -549,7 +549,7 @@ void launch_qr_cfg(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, 
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  TTC_CUDA(cudaLaunchKernelEx(&cfg, householder_qr_kernel<RMAX>, d_descs, csize, d_flags));
+  TTC_CUDA(cudaLaunchKernelEx(&cfg, householder_qr_kernel, d_descs, csize, d_flags));
   TTC_CHECK_LAUNCH();
 }
 }  // namespace
@@ -557,11 +557,7 @@ void launch_qr_cfg(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, 
 void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags) {
   if (count <= 0) return;
   TTC_REQUIRE(max_m <= QR_MAX_M, TTC_EDIM, "qr: row count exceeds the supported maximum (1536)");
-  // Register panels up to 512 rows; at 768 rows (24 rows per lane) the column and the loads in
-  // flight no longer fit the 128 registers of a 512-thread CTA and the shared-memory loop wins.
-  if (max_m <= 256) launch_qr_cfg<8>(d_descs, count, max_m, s, d_flags);
-  else if (max_m <= 512) launch_qr_cfg<16>(d_descs, count, max_m, s, d_flags);
-  else launch_qr_cfg<0>(d_descs, count, max_m, s, d_flags);
+  launch_qr_cfg(d_descs, count, max_m, s, d_flags);
 }
 
 }  // namespace ttc

@@ -121,6 +121,55 @@ static int op_kind(OpKind k) {
   }
 }
 
+// Algorithmic FLOPs of one launch at the sizes its descriptors run with.  Without device
+// bounds these are the capacity shapes the builder counts; with them (`val` reads a bound that
+// the run wrote), the bounded block: the QR, Q application and Jacobi of the SVD sweep work on
+// the rows left by the kept rank of the next bond, a GEMM with n_dev on its first *n_dev columns.
+static double qr_flops(double m, double n, bool with_q) {
+  const double k = std::min(m, n);
+  return (with_q ? 2.0 : 1.0) * (2.0 * m * k * k - 2.0 * k * k * k / 3.0) + 2.0 * m * k * (n - k);
+}
+static double qapply_flops(double m, double K, double nb) { return 4.0 * m * K * nb - 2.0 * K * K * nb; }
+static double jacobi_flops(double m, double n) { return 4.0 * m * n * n + 8.0 * n * n * n; }
+
+static double bounded_flops(const Plan& p, const Op& op, const std::function<int(const int*)>& val) {
+  const unsigned char* d = p.blob.data() + op.off;
+  auto bnd = [&](int cap, const int* ptr, int mult) {
+    return ptr ? std::min(cap, std::max(0, mult * val(ptr))) : cap;
+  };
+  double f = 0.0;
+  switch (op.kind) {
+    case OP_QR:
+      for (int i = 0; i < op.count; ++i) {
+        const QRDesc& q = ((const QRDesc*)d)[i];
+        f += qr_flops(bnd(q.m, q.m_dev, q.m_mult), bnd(q.n, q.n_dev, q.n_mult), q.Q != nullptr);
+      }
+      return f;
+    case OP_QAPPLY:
+      for (int i = 0; i < op.count; ++i) {
+        const QApplyDesc& q = ((const QApplyDesc*)d)[i];
+        const int m = bnd(q.m, q.m_dev, q.m_mult);
+        f += qapply_flops(m, std::min(q.K, m), bnd(q.nb, q.n_dev, 1));
+      }
+      return f;
+    case OP_JACOBI:
+      for (int i = 0; i < op.count; ++i) {
+        const JacobiDesc& j = ((const JacobiDesc*)d)[i];
+        const int m = bnd(j.m, j.m_dev, j.m_mult);
+        f += jacobi_flops(m, j.m_dev ? std::min(j.n, m) : j.n);   // a bounded factor is m x m at most
+      }
+      return f;
+    case OP_GEMM:
+      for (int i = 0; i < op.count; ++i) {
+        const GemmDesc& g = ((const GemmDesc*)d)[i];
+        f += 2.0 * g.m * bnd(g.n, g.n_dev, 1) * (double)g.k * std::max(1, g.batch);
+      }
+      return f;
+    default:
+      return op.flops;
+  }
+}
+
 // Profiled execution: an event pair around every launch, times accumulated per kernel family.
 static void run_plan_profiled(ttc_context* c, Plan& p) {
   std::vector<cudaEvent_t> ev;
@@ -148,6 +197,21 @@ static void run_plan_profiled(ttc_context* c, Plan& p) {
     ++i;
   }
   TTC_CUDA(cudaStreamSynchronize(c->stream));
+  // FLOPs at the sizes the launches ran with (device bounds read back once per address)
+  std::unordered_map<const int*, int> bound_cache;
+  auto val = [&](const int* ptr) {
+    auto it = bound_cache.find(ptr);
+    if (it != bound_cache.end()) return it->second;
+    int v = 0;
+    TTC_CUDA(cudaMemcpy(&v, ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    bound_cache[ptr] = v;
+    return v;
+  };
+  {
+    size_t j = 0;
+    for (const Op& op : p.ops)
+      if (op.kind != OP_STAGE) flops[j++] = bounded_flops(p, op, val);
+  }
   for (int k = 0; k < 8; ++k) { c->stats.kind_ms[k] = 0; c->stats.kind_launches[k] = 0; c->stats.kind_flops[k] = 0; }
   // TTC_PROFILE_TRACE=<file>: one line per launch appended (op kind, problems, the kernel-specific
   // size arguments a, b and total, device ms, algorithmic FLOPs)
@@ -310,10 +374,7 @@ void Builder::qr(const std::vector<QRDesc>& v) {
                 "qr: leading dims");
   }
   Op op; op.kind = OP_QR; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm; op.b = nn;
-  for (auto& d : v) {
-    const double m = d.m, k = std::min(d.m, d.n);
-    op.flops += (d.Q ? 2.0 : 1.0) * (2.0 * m * k * k - 2.0 * k * k * k / 3.0) + 2.0 * m * k * (d.n - k);
-  }
+  for (auto& d : v) op.flops += qr_flops(d.m, d.n, d.Q != nullptr);
   plan->ops.push_back(op);
 }
 void Builder::qapply(const std::vector<QApplyDesc>& v) {
@@ -329,7 +390,7 @@ void Builder::qapply(const std::vector<QApplyDesc>& v) {
     TTC_REQUIRE(d.lda >= d.m && d.ldb >= d.m && d.K <= d.m, TTC_EINTERNAL, "qr apply: leading dims");
   }
   Op op; op.kind = OP_QAPPLY; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm;
-  for (auto& d : v) op.flops += 4.0 * d.m * (double)d.K * d.nb - 2.0 * (double)d.K * d.K * d.nb;
+  for (auto& d : v) op.flops += qapply_flops(d.m, d.K, d.nb);
   plan->ops.push_back(op);
 }
 void Builder::jacobi(const std::vector<JacobiDesc>& v) {
@@ -348,7 +409,7 @@ void Builder::jacobi(const std::vector<JacobiDesc>& v) {
   }
   Op op; op.kind = OP_JACOBI; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm; op.b = nn;
   for (auto& d : v) op.total |= (d.W != nullptr);
-  for (auto& d : v) op.flops += 4.0 * d.m * (double)d.n * d.n + 8.0 * (double)d.n * d.n * d.n;
+  for (auto& d : v) op.flops += jacobi_flops(d.m, d.n);
   plan->ops.push_back(op);
 }
 void Builder::trunc(const std::vector<TruncDesc>& v, double tol, long long rmax) {
@@ -561,6 +622,7 @@ Plan* get_plan(ttc_context* c, const std::string& key, const std::function<void(
   TTC_CUDA(cudaMemcpy(p->d_blob, p->blob.data(), p->blob.size(), cudaMemcpyHostToDevice));
   p->ws_base = c->ws;
   Plan* raw = p.get();
+  c->stats.plans_built += 1;
   if (c->plans.size() > 64) c->plans.clear();
   c->plans[key] = std::move(p);
   return raw;

@@ -322,6 +322,43 @@ def test_batched_round_det_uneven_ranks():
             assert rel(got, ref) < 1e-10
 
 
+def test_repeated_rounds_reuse_their_plans():
+    """A repeated rounding with the same shapes reuses its execution plan (replayed as a CUDA
+    graph from the second run on) and gives bitwise the same result, for the deterministic
+    and the randomized rounding; new input values with the same ranks reuse it too."""
+    ctx = ttcuda.get_context()
+    dims = (2,) * 10
+    tts = [decaying_tt(dims, o.r_and_d_to_rks([1] + [10] * 9 + [1], dims), seed=400 + i, decay_per=2.0)
+           for i in range(3)]
+    xb = ttcuda.DeviceBatch.from_tts([to_dev(t) for t in tts])
+    rks = o.default_rank_heuristic(tts)
+    cap = ttcuda._rand_out_caps(dims, ttcuda._sketch_ranks(dims, rks, 64))
+    yr = ttcuda.DeviceBatch(dims, [cap] * 3)
+    yd = ttcuda.DeviceBatch(dims, [t.ttv_rks for t in tts])
+    runs = {"det": lambda: xb.round_det(yd, tol=1e-6),
+            "rand": lambda: xb.round_rand(yr, rks, seed=9, block_rks=64, precision="bf16", after_tol=1e-6)}
+    outs = {"det": yd, "rand": yr}
+    for name, run in runs.items():
+        run()
+        first = [np.concatenate([c.ravel() for c in t.ttv_vec]) for t in outs[name].download()]
+        built = ctx.stats()["plans_built"]
+        for _ in range(3):
+            run()
+            again = [np.concatenate([c.ravel() for c in t.ttv_vec]) for t in outs[name].download()]
+            assert all(np.array_equal(a, b) for a, b in zip(first, again)), name
+        assert ctx.stats()["plans_built"] == built, name
+    # same ranks, other values: same plans, results of the new input
+    tts2 = [decaying_tt(dims, t.ttv_rks, seed=500 + i, decay_per=2.0) for i, t in enumerate(tts)]
+    built = ctx.stats()["plans_built"]
+    xb.upload([to_dev(t) for t in tts2])
+    xb.round_det(yd, tol=1e-6)
+    assert ctx.stats()["plans_built"] == built
+    for t, got in zip(tts2, yd.download()):
+        ref = o.tt_rounding(t, tol=1e-6)
+        assert got.ttv_rks == ref.ttv_rks
+        assert rel(got, ref) < 1e-10
+
+
 def test_batched_round_rand_then_svd():
     dims = (2,) * 10
     tts = [decaying_tt(dims, o.r_and_d_to_rks([1] + [12] * 9 + [1], dims), seed=200 + i, decay_per=2.0)
