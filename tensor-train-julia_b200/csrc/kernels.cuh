@@ -60,8 +60,12 @@ struct JacobiDesc {
   int* info;        // optional: sweeps used (negative if the sweep cap was hit)
   const int* m_dev; int m_mult;   // optional: rows >= m_mult * *m_dev of X are zero
 };
+// `order` (count ints of device workspace, or nullptr): the launch first ranks the problems by
+// their size (rows after the device bound x columns^2, largest first) so that the clusters,
+// which the hardware starts in index order, take the longest problems first.
+constexpr int kJacobiOrderMax = 4096;
 void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, bool accw, cudaStream_t s,
-                   int* d_flags);
+                   int* d_flags, int* order = nullptr);
 
 // ---- truncation rule (tt_kernels.cu): floor(s, tol) then min(k, rmax, #(s>0))
 struct TruncDesc {

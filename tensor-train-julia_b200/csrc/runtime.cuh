@@ -34,6 +34,7 @@ struct Op {
   double tol = 0.0;
   long long rmax = 0;
   double flops = 0.0;  // algorithmic FLOPs of the launch (profiling only)
+  int* iw = nullptr;   // kernel-specific device int workspace (the Jacobi problem order)
 };
 
 // "Finalize" descriptor: if *flag != 0, zero the TT's cores and restore its ranks.

@@ -346,14 +346,16 @@ __host__ __device__ __forceinline__ size_t dyn_doubles(int bw, int ms, int n, bo
 // within 128 registers so that two CTAs share an SM.
 template <int RMAX>
 __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
-    jacobi_svd_kernel(const JacobiDesc* __restrict__ descs, int bw, int csize, int* flags) {
+    jacobi_svd_kernel(const JacobiDesc* __restrict__ descs, const int* __restrict__ order, int bw, int csize,
+                      int* flags) {
   extern __shared__ double sm[];
   __shared__ int s_any, s_nact;
   __shared__ double s_red[NW];
   __shared__ double s_scr[32 + 4 * 64];
   cg::cluster_group cluster = cg::this_cluster();
   const int crank = (int)cluster.block_rank();
-  const JacobiDesc D = descs[blockIdx.x / csize];
+  const int prob = (int)(blockIdx.x / csize);
+  const JacobiDesc D = descs[order ? order[prob] : prob];
   if (D.m <= 0 || D.n <= 0) return;             // uniform across the cluster
   // rows beyond the device bound are zero and stay zero under the rotations (at least one row
   // is kept so that an all-zero problem still reports its zero singular values)
@@ -506,6 +508,26 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   }
 }
 
+// Problem order of a launch: by decreasing size m x n^2, m the rows left by the device bound and
+// n the columns (at most m when bounded: the bounded factor is square), ties by index.
+__global__ void jacobi_order_kernel(const JacobiDesc* __restrict__ descs, int count, int* __restrict__ order) {
+  for (int i = threadIdx.x; i < count; i += blockDim.x) {
+    auto key = [&](int j) {
+      const JacobiDesc& d = descs[j];
+      const double m = dev_bound(d.m, d.m_dev, d.m_mult);
+      const double n = d.m_dev ? fmin((double)d.n, m) : (double)d.n;
+      return m * n * n;
+    };
+    const double ki = key(i);
+    int rank = 0;
+    for (int j = 0; j < count; ++j) {
+      const double kj = key(j);
+      rank += (kj > ki) || (kj == ki && j < i);
+    }
+    order[rank] = i;
+  }
+}
+
 namespace {
 int sm_count() {
   static int dev_cached = -1, count = 0;
@@ -531,16 +553,23 @@ static int jacobi_bw(int max_m, int max_n, bool accw, size_t* smem_out) {
   return bw;
 }
 
+// Cluster size of an ordered launch (measured on the 64-TT rounding: 8 for the two-CTA-per-SM
+// instance, 4 for the one-CTA-per-SM instance; 8 there runs 3.5 waves and loses).
 template <int RMAX>
-static int jacobi_cluster_size(int count, int max_n, int bw, size_t smem) {
+constexpr int kOrderedCsize = RMAX <= 8 ? 8 : 4;
+template <int RMAX>
+static int jacobi_cluster_size(int count, int max_n, int bw, size_t smem, bool ordered) {
   // CTAs per problem: fill the SMs (resident CTAs per SM from registers and shared memory),
-  // at most 8 (portable cluster size) and at most the disjoint block pairs of a round.
+  // at most 8 (portable cluster size) and at most the disjoint block pairs of a round.  With
+  // the problems ordered largest first the grid may exceed the resident slots (the clusters
+  // that start later take the smaller problems): then at least kOrderedCsize<RMAX>.
   int per_sm = 1;
   TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_svd_kernel<RMAX>, NT, smem));
   per_sm = std::max(1, per_sm);
   const int slots = sm_count() * per_sm;
   const int pairs = std::max(1, ((max_n + bw - 1) / bw + 1) / 2);
   int c = std::max(1, slots / std::max(1, count));
+  if (ordered) c = std::max(c, kOrderedCsize<RMAX>);
   c = std::min(c, std::min(8, pairs));
   int p2 = 1;
   while (p2 * 2 <= c) p2 *= 2;
@@ -549,7 +578,7 @@ static int jacobi_cluster_size(int count, int max_n, int bw, size_t smem) {
 
 template <int RMAX>
 static void launch_jacobi_t(const JacobiDesc* d_descs, int count, int max_n, int bw, size_t smem, cudaStream_t s,
-                            int* d_flags) {
+                            int* d_flags, int* order) {
   static int attr_dev = -1;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -557,7 +586,11 @@ static void launch_jacobi_t(const JacobiDesc* d_descs, int count, int max_n, int
     TTC_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel<RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     attr_dev = dev;
   }
-  const int csize = jacobi_cluster_size<RMAX>(count, max_n, bw, smem);
+  if (order) {
+    jacobi_order_kernel<<<1, 512, 0, s>>>(d_descs, count, order);
+    TTC_CHECK_LAUNCH();
+  }
+  const int csize = jacobi_cluster_size<RMAX>(count, max_n, bw, smem, order != nullptr);
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)(count * csize));
   cfg.blockDim = dim3(NT);
@@ -570,18 +603,19 @@ static void launch_jacobi_t(const JacobiDesc* d_descs, int count, int max_n, int
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  TTC_CUDA(cudaLaunchKernelEx(&cfg, jacobi_svd_kernel<RMAX>, d_descs, bw, csize, d_flags));
+  TTC_CUDA(cudaLaunchKernelEx(&cfg, jacobi_svd_kernel<RMAX>, d_descs, (const int*)order, bw, csize, d_flags));
   TTC_CHECK_LAUNCH();
 }
 
 void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, bool accw, cudaStream_t s,
-                   int* d_flags) {
+                   int* d_flags, int* order) {
   if (count <= 0) return;
   size_t smem = 0;
   const int bw = jacobi_bw(max_m, max_n, accw, &smem);
   TTC_REQUIRE(smem <= 200 * 1024, TTC_EDIM, "jacobi: matrix too large for the shared-memory blocks");
-  if (max_m <= 256) launch_jacobi_t<8>(d_descs, count, max_n, bw, smem, s, d_flags);
-  else launch_jacobi_t<16>(d_descs, count, max_n, bw, smem, s, d_flags);
+  if (count > kJacobiOrderMax) order = nullptr;
+  if (max_m <= 256) launch_jacobi_t<8>(d_descs, count, max_n, bw, smem, s, d_flags, order);
+  else launch_jacobi_t<16>(d_descs, count, max_n, bw, smem, s, d_flags, order);
 }
 
 }  // namespace ttc
