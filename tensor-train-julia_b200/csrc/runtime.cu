@@ -105,7 +105,7 @@ static void launch_op(ttc_context* c, const Plan& p, const Op& op) {
 
 long long count_launches(const Plan& p) {
   long long n = 0;
-  for (const Op& op : p.ops) n += (op.kind != OP_STAGE);
+  for (const Op& op : p.ops) n += (op.kind != OP_STAGE) + (op.kind == OP_JACOBI && op.iw ? 1 : 0);   // + order kernel
   return n;
 }
 
