@@ -149,7 +149,14 @@ int ttc_batch_destroy(ttc_batch* b);
 /* TTvector(N, vec, dims, rks, ot) constructor, src/tt_tools.jl:24-34: uploads one TT. */
 int ttc_batch_upload(ttc_batch* b, int32_t index, const ttc_ttv* x);
 int ttc_batch_download(ttc_batch* b, int32_t index, ttc_ttv_out* y);
-/* Upload/download all `count` TTs of the batch in one staged transfer each. */
+/* Page-locked host memory mapped into the device address space (no counterpart in the
+ * reference; a Julia caller would pass pinned CUDA.jl host arrays).  TT cores in such memory
+ * skip the copy through the library's pinned staging buffer: uploads are DMA copies straight
+ * to the device (one per run of cores adjacent in memory), downloads are written by the layout
+ * kernel over the host link.  Pageable cores are staged. */
+int ttc_host_alloc(size_t bytes, void** out);
+int ttc_host_free(void* p);
+/* Upload/download all `count` TTs of the batch in one transfer each. */
 int ttc_batch_upload_all(ttc_batch* b, const ttc_ttv* xs);
 int ttc_batch_download_all(ttc_batch* b, ttc_ttv_out* ys);
 int ttc_batch_ranks(ttc_batch* b, int32_t index, int64_t* rks /* N+1 */);

@@ -95,7 +95,25 @@ void validate_ttv(const ttc_ttv* x) {
   for (int k = 0; k <= x->N; ++k) TTC_REQUIRE(x->rks[k] >= 1, TTC_EDIM, "TTvector: ranks must be >= 1");
 }
 
-// Upload many TTs into consecutive slots [first, first+m) of a batch.
+// Device address of the host range [p, p + bytes) when all of it lies in page-locked host
+// memory mapped into the device address space (cudaHostAlloc, cudaHostRegister), so that a
+// kernel can read or write it directly over the host link; nullptr otherwise (pageable memory).
+static const void* mapped_host_view(const void* p, size_t bytes) {
+  if (!p || bytes == 0) return nullptr;
+  cudaPointerAttributes a{}, e{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+  const char* last = (const char*)p + bytes - 1;
+  if (cudaPointerGetAttributes(&e, last) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  if (e.type != cudaMemoryTypeHost || !e.devicePointer) return nullptr;
+  if ((const char*)e.devicePointer - (const char*)a.devicePointer != (std::ptrdiff_t)(bytes - 1)) return nullptr;
+  return a.devicePointer;
+}
+
+// Upload many TTs into consecutive slots [first, first+m) of a batch.  Cores in page-locked
+// memory are copied by DMA straight into the device staging area, one copy per run of cores
+// adjacent in host memory; pageable cores are first packed into the context's pinned buffer.
+// A layout kernel then moves the staged cores into the batch slots.
 void batch_upload_many(ttc_batch* b, int first, int m, const ttc_ttv* xs, bool reverse) {
   ttc_context* c = b->ctx;
   const int N = b->N;
@@ -110,6 +128,12 @@ void batch_upload_many(ttc_batch* b, int first, int m, const ttc_ttv* xs, bool r
       TTC_REQUIRE(x.rks[reverse ? N - k : k] <= b->capr(first + i, k), TTC_EDIM, "upload: rank exceeds the batch capacity");
     for (int k = 0; k < N; ++k) data += (size_t)x.dims[k] * x.rks[k] * x.rks[k + 1];
   }
+  bool direct = true;   // every core page-locked (validated above)
+  for (int i = 0; i < m && direct; ++i)
+    for (int k = 0; k < N && direct; ++k) {
+      const size_t cnt = (size_t)xs[i].dims[k] * xs[i].rks[k] * xs[i].rks[k + 1];
+      direct = mapped_host_view(xs[i].cores[k], cnt * sizeof(double)) != nullptr;
+    }
   const size_t nd = (size_t)m * N;
   const size_t off_desc = align_up(data * sizeof(double), 256);
   const size_t off_rk = align_up(off_desc + nd * sizeof(CopyDesc), 256);
@@ -146,13 +170,23 @@ void batch_upload_many(ttc_batch* b, int first, int m, const ttc_ttv* xs, bool r
   // running while the next one is staged; then the descriptors and ranks
   TTC_CUDA(cudaMemsetAsync(b->core(first, 0), 0, sizeof(double) * (b->tt_off[first + m] - b->tt_off[first]), c->stream));
   size_t sent = 0;
-  for (size_t gi = 0; gi < hcp.size();) {
-    size_t gj = gi, bytes = 0;
-    while (gj < hcp.size() && (gj == gi || bytes < kStageChunk)) bytes += hcp[gj++].bytes;
-    parallel_memcpy(std::vector<HostCopy>(hcp.begin() + (long)gi, hcp.begin() + (long)gj));
-    TTC_CUDA(cudaMemcpyAsync(d + sent, h + sent, bytes, cudaMemcpyHostToDevice, c->stream));
-    sent += bytes;
-    gi = gj;
+  if (direct) {
+    for (size_t gi = 0; gi < hcp.size();) {      // runs of cores adjacent in host memory
+      size_t gj = gi + 1, bytes = hcp[gi].bytes;
+      while (gj < hcp.size() && (const char*)hcp[gj].src == (const char*)hcp[gi].src + bytes) bytes += hcp[gj++].bytes;
+      TTC_CUDA(cudaMemcpyAsync(d + sent, hcp[gi].src, bytes, cudaMemcpyHostToDevice, c->stream));
+      sent += bytes;
+      gi = gj;
+    }
+  } else {
+    for (size_t gi = 0; gi < hcp.size();) {
+      size_t gj = gi, bytes = 0;
+      while (gj < hcp.size() && (gj == gi || bytes < kStageChunk)) bytes += hcp[gj++].bytes;
+      parallel_memcpy(std::vector<HostCopy>(hcp.begin() + (long)gi, hcp.begin() + (long)gj));
+      TTC_CUDA(cudaMemcpyAsync(d + sent, h + sent, bytes, cudaMemcpyHostToDevice, c->stream));
+      sent += bytes;
+      gi = gj;
+    }
   }
   TTC_CUDA(cudaMemcpyAsync(d + off_desc, h + off_desc, total - off_desc, cudaMemcpyHostToDevice, c->stream));
   launch_copy((const CopyDesc*)(d + off_desc), (int)ci, maxe, c->stream);
@@ -185,6 +219,17 @@ void batch_download_many(ttc_batch* b, int first, int m, ttc_ttv_out* ys, bool r
                     "download: output capacity smaller than the result rank");
     for (int k = 0; k < N; ++k) data += (size_t)b->dims[k] * b->rk(t, k) * b->rk(t, k + 1);
   }
+  // output cores in mapped page-locked memory are written by the layout kernel itself
+  std::vector<void*> views;
+  bool direct = true;
+  for (int i = 0; i < m && direct; ++i)
+    for (int ko = 0; ko < N && direct; ++ko) {
+      const int k = reverse ? N - 1 - ko : ko;
+      const size_t cnt = (size_t)b->dims[k] * b->rk(first + i, k) * b->rk(first + i, k + 1);
+      views.push_back(const_cast<void*>(mapped_host_view(ys[i].cores[ko], cnt * sizeof(double))));
+      direct = views.back() != nullptr;
+    }
+  if (direct) data = 0;
   const size_t nd = (size_t)m * N;
   const size_t off_desc = align_up(data * sizeof(double), 256);
   const size_t total = off_desc + nd * sizeof(CopyDesc);
@@ -200,55 +245,60 @@ void batch_download_many(ttc_batch* b, int first, int m, ttc_ttv_out* ys, bool r
     for (int ko = 0; ko < N; ++ko) {           // output core ko
       const int k = reverse ? N - 1 - ko : ko;  // batch core holding it
       const long long n = b->dims[k], r0 = b->rk(t, k), r1 = b->rk(t, k + 1), cap0 = b->capr(t, k);
+      double* dst = direct ? (double*)views[(size_t)i * N + ko] : (double*)d + o;
       if (!reverse)
-        hc[ci++] = cd3(b->core(t, k), (double*)d + o, n, r0, r1, cap0, 1, cap0 * n, 1, n, n * r0);
+        hc[ci++] = cd3(b->core(t, k), dst, n, r0, r1, cap0, 1, cap0 * n, 1, n, n * r0);
       else  // output (i, a, b) with a < r1, b < r0 from internal (b, i, a)
-        hc[ci++] = cd3(b->core(t, k), (double*)d + o, n, r1, r0, cap0, cap0 * n, 1, 1, n, n * r1);
+        hc[ci++] = cd3(b->core(t, k), dst, n, r1, r0, cap0, cap0 * n, 1, 1, n, n * r1);
       maxe = std::max<long long>(maxe, n * r0 * r1);
       offs.push_back(o);
-      o += (size_t)n * r0 * r1;
+      if (!direct) o += (size_t)n * r0 * r1;
     }
   }
   TTC_CUDA(cudaMemcpyAsync(d + off_desc, h + off_desc, nd * sizeof(CopyDesc), cudaMemcpyHostToDevice, c->stream));
   launch_copy((const CopyDesc*)(d + off_desc), (int)ci, maxe, c->stream);
-  size_t q = 0;
-  std::vector<HostCopy> hcp;
-  for (int i = 0; i < m; ++i) {
-    const int t = first + i;
-    for (int ko = 0; ko < N; ++ko) {
-      const int k = reverse ? N - 1 - ko : ko;
-      const size_t cnt = (size_t)b->dims[k] * b->rk(t, k) * b->rk(t, k + 1);
-      hcp.push_back({ys[i].cores[ko], (double*)h + offs[q++], cnt * sizeof(double)});
+  if (direct) {
+    TTC_CUDA(cudaStreamSynchronize(c->stream));
+  } else {
+    size_t q = 0;
+    std::vector<HostCopy> hcp;
+    for (int i = 0; i < m; ++i) {
+      const int t = first + i;
+      for (int ko = 0; ko < N; ++ko) {
+        const int k = reverse ? N - 1 - ko : ko;
+        const size_t cnt = (size_t)b->dims[k] * b->rk(t, k) * b->rk(t, k + 1);
+        hcp.push_back({ys[i].cores[ko], (double*)h + offs[q++], cnt * sizeof(double)});
+      }
     }
-  }
-  // transfer chunk by chunk, an event after each; unpack a chunk while the next ones arrive
-  std::vector<std::pair<size_t, size_t>> groups;   // [gi, gj) of hcp
-  std::vector<cudaEvent_t> evs;
-  size_t sent = 0;
-  try {
-    for (size_t gi = 0; gi < hcp.size();) {
-      size_t gj = gi, bytes = 0;
-      while (gj < hcp.size() && (gj == gi || bytes < kStageChunk)) bytes += hcp[gj++].bytes;
-      cudaEvent_t e;
-      TTC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      evs.push_back(e);
-      TTC_CUDA(cudaMemcpyAsync(h + sent, d + sent, bytes, cudaMemcpyDeviceToHost, c->stream));
-      TTC_CUDA(cudaEventRecord(e, c->stream));
-      groups.push_back({gi, gj});
-      sent += bytes;
-      gi = gj;
+    // transfer chunk by chunk, an event after each; unpack a chunk while the next ones arrive
+    std::vector<std::pair<size_t, size_t>> groups;   // [gi, gj) of hcp
+    std::vector<cudaEvent_t> evs;
+    size_t sent = 0;
+    try {
+      for (size_t gi = 0; gi < hcp.size();) {
+        size_t gj = gi, bytes = 0;
+        while (gj < hcp.size() && (gj == gi || bytes < kStageChunk)) bytes += hcp[gj++].bytes;
+        cudaEvent_t e;
+        TTC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        evs.push_back(e);
+        TTC_CUDA(cudaMemcpyAsync(h + sent, d + sent, bytes, cudaMemcpyDeviceToHost, c->stream));
+        TTC_CUDA(cudaEventRecord(e, c->stream));
+        groups.push_back({gi, gj});
+        sent += bytes;
+        gi = gj;
+      }
+      for (size_t g = 0; g < groups.size(); ++g) {
+        TTC_CUDA(cudaEventSynchronize(evs[g]));
+        parallel_memcpy(std::vector<HostCopy>(hcp.begin() + (long)groups[g].first, hcp.begin() + (long)groups[g].second));
+      }
+    } catch (...) {
+      cudaStreamSynchronize(c->stream);
+      for (auto e : evs) cudaEventDestroy(e);
+      throw;
     }
-    for (size_t g = 0; g < groups.size(); ++g) {
-      TTC_CUDA(cudaEventSynchronize(evs[g]));
-      parallel_memcpy(std::vector<HostCopy>(hcp.begin() + (long)groups[g].first, hcp.begin() + (long)groups[g].second));
-    }
-  } catch (...) {
-    cudaStreamSynchronize(c->stream);
+    TTC_CUDA(cudaStreamSynchronize(c->stream));
     for (auto e : evs) cudaEventDestroy(e);
-    throw;
   }
-  TTC_CUDA(cudaStreamSynchronize(c->stream));
-  for (auto e : evs) cudaEventDestroy(e);
   for (int i = 0; i < m; ++i) {
     const int t = first + i;
     for (int k = 0; k <= N; ++k) ys[i].rks[k] = b->rk(t, reverse ? N - k : k);
@@ -458,6 +508,30 @@ int ttc_batch_upload(ttc_batch* b, int32_t index, const ttc_ttv* x) {
     TTC_REQUIRE(index >= 0 && index < b->count, TTC_EARG, "upload: index out of range");
     batch_upload_many(b, index, 1, x);
   });
+}
+
+int ttc_host_alloc(size_t bytes, void** out) {
+  if (!out || bytes == 0) return TTC_EARG;
+  *out = nullptr;
+  const cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    ttc::set_noctx_error(std::string("ttc_host_alloc: ") + cudaGetErrorString(e));
+    return TTC_ENOMEM;
+  }
+  return TTC_OK;
+}
+
+int ttc_host_free(void* p) {
+  if (!p) return TTC_OK;
+  const cudaError_t e = cudaFreeHost(p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ttc::set_noctx_error(std::string("ttc_host_free: ") + cudaGetErrorString(e));
+    return TTC_ECUDA;
+  }
+  return TTC_OK;
 }
 
 int ttc_batch_upload_all(ttc_batch* b, const ttc_ttv* xs) {

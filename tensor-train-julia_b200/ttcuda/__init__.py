@@ -11,6 +11,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 from typing import List, Optional, Sequence
+import weakref
 
 import numpy as np
 
@@ -216,17 +217,51 @@ def _tto(A: TToperator, keep: _Keep) -> L.TTO:
     return L.TTO(A.N, _i64(A.tto_dims, keep), _i64(A.tto_rks, keep), _ptrs(cores, keep))
 
 
-class _Out:
-    """Caller-allocated output buffers at the stated capacities (ttc_ttv_out)."""
+def host_empty(n: int, dtype=np.float64) -> np.ndarray:
+    """A 1-D array of n elements in page-locked host memory mapped into the device address space
+    (ttc_host_alloc), freed when the array and its views are gone.  TT cores in such memory are
+    uploaded by DMA without the staging copy and written directly by the download kernel."""
+    nbytes = max(1, int(n) * np.dtype(dtype).itemsize)
+    p = C.c_void_p()
+    st = lib.ttc_host_alloc(C.c_size_t(nbytes), C.byref(p))
+    if st != 0:
+        raise MemoryError(f"ttc_host_alloc({nbytes}): {lib.ttc_last_error(None).decode()}")
+    buf = (C.c_char * nbytes).from_address(p.value)
+    weakref.finalize(buf, lib.ttc_host_free, C.c_void_p(p.value))
+    return np.frombuffer(buf, dtype=dtype, count=int(n))
 
-    def __init__(self, dims, caps):
+
+def pinned_tt(x: "TTvector") -> "TTvector":
+    """A copy of x whose cores lie in one page-locked block (host_empty): one DMA per upload."""
+    sizes = [int(np.prod(c.shape)) for c in x.ttv_vec]
+    flat = host_empty(sum(sizes))
+    vec, o = [], 0
+    for c, s in zip(x.ttv_vec, sizes):
+        v = flat[o:o + s].reshape(c.shape, order="F")
+        v[...] = c
+        vec.append(v)
+        o += s
+    return TTvector(x.N, vec, x.ttv_dims, x.ttv_rks, x.ttv_ot)
+
+
+class _Out:
+    """Caller-allocated output buffers at the stated capacities (ttc_ttv_out); `pinned` puts the
+    cores in one page-locked block, which the download kernel writes directly."""
+
+    def __init__(self, dims, caps, pinned: bool = False):
         self.N = len(dims)
         self.dims = tuple(int(n) for n in dims)
         self.keep = _Keep()
         self.caps = np.asarray(caps, dtype=np.int64)
         self.rks = np.zeros(self.N + 1, dtype=np.int64)
         self.ot = np.zeros(self.N, dtype=np.int64)
-        self.bufs = [np.empty(int(self.dims[k] * self.caps[k] * self.caps[k + 1]), dtype=np.float64) for k in range(self.N)]
+        sizes = [int(self.dims[k] * self.caps[k] * self.caps[k + 1]) for k in range(self.N)]
+        if pinned:
+            flat = host_empty(sum(sizes))
+            offs = np.concatenate([[0], np.cumsum(sizes)])
+            self.bufs = [flat[offs[k]:offs[k + 1]] for k in range(self.N)]
+        else:
+            self.bufs = [np.empty(sizes[k], dtype=np.float64) for k in range(self.N)]
         self.s = L.TTVOut(self.N, self.caps.ctypes.data_as(L.P_i64), self.rks.ctypes.data_as(L.P_i64),
                           self.ot.ctypes.data_as(L.P_i64), _ptrs(self.bufs, self.keep))
 
@@ -536,11 +571,12 @@ class DeviceBatch:
     def download(self, reuse: bool = False) -> List[TTvector]:
         """The batch's TTs as host TTvectors.  With reuse=True the host buffers of the previous
         reusing download are written again (no allocation; the TTvectors it returned then see
-        the new values), as a loop that rounds and downloads the same basis repeatedly wants."""
+        the new values), as a loop that rounds and downloads the same basis repeatedly wants;
+        those buffers are page-locked, so the download kernel writes them directly."""
         if reuse:
             outs = getattr(self, "_outs", None)
             if outs is None:
-                outs = self._outs = [_Out(self.dims, c) for c in self.caps]
+                outs = self._outs = [_Out(self.dims, c, pinned=True) for c in self.caps]
         else:
             outs = [_Out(self.dims, c) for c in self.caps]
         arr = (L.TTVOut * len(outs))(*[o.s for o in outs])

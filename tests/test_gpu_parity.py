@@ -359,6 +359,26 @@ def test_repeated_rounds_reuse_their_plans():
         assert rel(got, ref) < 1e-10
 
 
+def test_page_locked_upload_and_download_match_staged():
+    """Cores in page-locked host memory skip the staging copy (uploads by DMA, downloads written
+    by the layout kernel); the results equal those through the staging buffer."""
+    dims = (2, 3, 2, 4, 2, 3)
+    tts = [decaying_tt(dims, o.r_and_d_to_rks([1, 2, 5, 7, 6, 3, 1], dims), seed=600 + i, decay_per=2.0)
+           for i in range(4)]
+    dev = [to_dev(t) for t in tts]
+    xs = ttcuda.DeviceBatch.from_tts(dev)
+    xp = ttcuda.DeviceBatch.from_tts([ttcuda.pinned_tt(t) for t in dev])
+    for a, b in zip(xs.download(), xp.download(reuse=True)):
+        assert a.ttv_rks == b.ttv_rks
+        assert all(np.array_equal(u, v) for u, v in zip(a.ttv_vec, b.ttv_vec))
+    ys = ttcuda.DeviceBatch(dims, [t.ttv_rks for t in tts])
+    xp.round_det(ys, tol=1e-4)
+    staged, pinned = ys.download(), ys.download(reuse=True)
+    for t, a, b in zip(tts, staged, pinned):
+        assert a.ttv_rks == b.ttv_rks == o.tt_rounding(t, tol=1e-4).ttv_rks
+        assert all(np.array_equal(u, v) for u, v in zip(a.ttv_vec, b.ttv_vec))
+
+
 def test_batched_round_rand_then_svd():
     dims = (2,) * 10
     tts = [decaying_tt(dims, o.r_and_d_to_rks([1] + [12] * 9 + [1], dims), seed=200 + i, decay_per=2.0)
