@@ -35,9 +35,11 @@ sys.path.insert(0, os.path.join(ROOT, "tensor-train-julia_b200"))
 
 D, NPHYS, BATCH, RMIN, RMAX, TOL = 32, 2, 64, 16, 256, 1e-8
 METRIC = "TT roundings/s at d=32,r=256: mixed vs FP64 GPU at 1e-8 rel err; % roofline"
-# DRAM bytes (read + write) of one mixed-step Householder QR launch over 16 TTs, measured with
-# `ncu --set full` on this kernel: 38.0 MB + 24.1 MB.
-QR_DRAM_BYTES_16TT = 62.13e6
+# DRAM bytes (read + write) per launch of the QR family (householder_qr_kernel and
+# householder_apply_q_kernel, 123 launches) in one mixed step of the 64-TT workload, mean over the
+# launches of an ncu capture of that step (dram__bytes_read.sum + dram__bytes_write.sum): 99.7 GB
+# over 123 launches.  Other batch sizes change the L2 residency, so no scaled figure is given.
+QR_FAMILY_DRAM_BYTES_PER_LAUNCH_64TT = 810.7e6
 
 
 # ------------------------------------------------------------------------- workload
@@ -384,9 +386,11 @@ def main():
                              "fp64_algorithmic": flops_fp64 * world * args.steps / (ms_fp64 / 1e3) / 1e9},
             "roofline": {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": fp64_peak_tflops,
                          "unit": "TFLOP/s", "frac": (achieved / fp64_peak_tflops) if achieved else None,
-                         "traffic": (QR_DRAM_BYTES_16TT * len(tts) / 16.0) if dom == "householder_qr" else None,
-                         "traffic_note": "dram read+write of one mixed-step QR launch (768-row panels) in the 16-TT "
-                                         "ncu capture, scaled by TTs per launch",
+                         "traffic": (QR_FAMILY_DRAM_BYTES_PER_LAUNCH_64TT
+                                     if dom == "householder_qr" and len(tts) == 64 else None),
+                         "traffic_note": "mean dram read+write per QR-family launch of one 64-TT mixed step (ncu "
+                                         "capture of that step); the 768-row randomized-sweep QRs carry it: "
+                                         "input and Q exceed L2",
                          "peak_source": "FP64 cuBLAS DGEMM 4096^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
                          "avg_launch_ms": dom_avg_ms, "launches_per_step": dom_n,
                          "profile_ms_per_step": {k: round(v[0], 3) for k, v in prof_m.items() if v[1]},
