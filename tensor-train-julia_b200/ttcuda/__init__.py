@@ -64,6 +64,9 @@ class TTvector:
             if c.shape != (self.ttv_dims[k], self.ttv_rks[k], self.ttv_rks[k + 1]):
                 raise DimensionMismatch(f"TTvector: core {k + 1} has shape {c.shape}")
 
+    def __getstate__(self):   # copies and pickles leave out the cached ctypes marshalling
+        return {k: v for k, v in self.__dict__.items() if k != "_marshal"}
+
     def copy(self) -> "TTvector":
         return TTvector(self.N, [c.copy(order="F") for c in self.ttv_vec], self.ttv_dims, self.ttv_rks, self.ttv_ot)
 
@@ -199,21 +202,36 @@ def _i64(v, keep: _Keep):
 
 
 def _ptrs(arrays, keep: _Keep):
-    arr = (L.P_f64 * len(arrays))()
-    for i, a in enumerate(arrays):
-        keep.append(a)
-        arr[i] = a.ctypes.data_as(L.P_f64)
+    keep.extend(arrays)
+    arr = (C.c_void_p * len(arrays))(*[a.__array_interface__["data"][0] for a in arrays])
     keep.append(arr)
     return C.cast(arr, L.PP_f64)
 
 
+def _f64_fortran(c):
+    """c itself when it is already a Fortran-ordered float64 array, else a converted copy."""
+    if isinstance(c, np.ndarray) and c.dtype == np.float64 and c.flags.f_contiguous:
+        return c
+    return np.asfortranarray(c, dtype=np.float64)
+
+
 def _ttv(x: TTvector, keep: _Keep) -> L.TTV:
-    cores = [np.asfortranarray(c, dtype=np.float64) for c in x.ttv_vec]
-    return L.TTV(x.N, _i64(x.ttv_dims, keep), _i64(x.ttv_rks, keep), _i64(x.ttv_ot, keep), _ptrs(cores, keep))
+    # the marshalled arrays are cached on x while its core arrays (held by the cache, so their
+    # ids stay unique) and its dims/ranks/ot are the same; in-place core updates keep them valid
+    key = (tuple(map(id, x.ttv_vec)), tuple(x.ttv_dims), tuple(x.ttv_rks), tuple(x.ttv_ot))
+    cached = getattr(x, "_marshal", None)
+    if cached is None or cached[0] != key:
+        ck = _Keep()
+        cores = [_f64_fortran(c) for c in x.ttv_vec]
+        args = (_i64(x.ttv_dims, ck), _i64(x.ttv_rks, ck), _i64(x.ttv_ot, ck), _ptrs(cores, ck))
+        cached = (key, args, ck, list(x.ttv_vec))
+        x._marshal = cached
+    keep.append(cached)
+    return L.TTV(x.N, *cached[1])
 
 
 def _tto(A: TToperator, keep: _Keep) -> L.TTO:
-    cores = [np.asfortranarray(c, dtype=np.float64) for c in A.tto_vec]
+    cores = [_f64_fortran(c) for c in A.tto_vec]
     return L.TTO(A.N, _i64(A.tto_dims, keep), _i64(A.tto_rks, keep), _ptrs(cores, keep))
 
 
