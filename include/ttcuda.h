@@ -38,7 +38,7 @@ typedef enum {
 } ttc_status;
 
 enum { TTC_DIR_LEFT = 0, TTC_DIR_RIGHT = 1 };         /* direction=:left / :right      */
-enum { TTC_PREC_FP64 = 0, TTC_PREC_BF16 = 1 };        /* sketch-contraction precision  */
+enum { TTC_PREC_FP64 = 0, TTC_PREC_BF16 = 1, TTC_PREC_TF32 = 2 };   /* sketch-contraction precision */
 
 typedef struct ttc_context ttc_context;
 typedef struct ttc_batch ttc_batch;
@@ -89,7 +89,7 @@ typedef struct {
   int32_t orthogonal;
   uint64_t seed;
   int64_t block_rks;            /* <= 0 means N (the reference default)  */
-  int32_t precision;            /* TTC_PREC_FP64 or TTC_PREC_BF16         */
+  int32_t precision;            /* TTC_PREC_FP64, _BF16 or _TF32 (FP32 operands read as TF32 by the tensor cores) */
   const double* const* sketch_blocks;
 } ttc_sketch_opts;
 

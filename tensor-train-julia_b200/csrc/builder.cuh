@@ -37,8 +37,10 @@ struct Builder {
   void sumsq(const std::vector<NormDesc>& v);
   void apply(const std::vector<ApplyDesc>& v);
   void philox(const std::vector<PhiloxDesc>& v);
-  void bf16gemm(std::vector<Bf16GemmDesc> v);
-  void cvt_bf16(const std::vector<CvtDesc>& v);
+  // tcgen05 GEMM of BF16 operands, or FP32 operands read as TF32 (tf32 = true)
+  void bf16gemm(std::vector<Bf16GemmDesc> v, bool tf32 = false);
+  // FP64 -> BF16, or FP64 -> FP32 rounded to TF32 (f32 = true)
+  void cvt_bf16(const std::vector<CvtDesc>& v, bool f32 = false);
   void zerochk(const std::vector<ZeroChkDesc>& v);
   void finalize(const std::vector<FinalDesc>& v);
   void setrank(const std::vector<SetRankDesc>& v);

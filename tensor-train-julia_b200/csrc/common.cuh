@@ -67,4 +67,14 @@ struct GemmDesc {
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
+// FP32 value rounded to the nearest TF32 (10-bit mantissa, PTX cvt.rna.tf32.f32).  The tensor
+// cores read a kind::tf32 operand by dropping its low 13 mantissa bits (toward zero); operands
+// rounded here first carry an unbiased error instead, which does not accumulate coherently
+// through the levels of a recursive sketch.
+__device__ __forceinline__ float round_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
 }  // namespace ttc

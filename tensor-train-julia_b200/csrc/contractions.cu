@@ -152,6 +152,7 @@ void emit_sketch_op_f64(Builder& B, const DevTTO& H, ttc_batch* x, int t, const 
 // A y - b (:169-214, here alpha = [1, -1]).  Term 0 is A*ys[0] when A is given.
 void rand_rounding_general(ttc_context* c, int m, const double* alpha, const ttc_tto* Ah, const ttc_ttv* ys,
                            const int64_t* rks, const ttc_sketch_opts& sk, ttc_ttv_out* y) {
+  check_precision(sk.precision);
   TTC_REQUIRE(m >= 1, TTC_EARG, "ttrand_rounding: empty combination");
   const int N = ys[0].N;
   for (int j = 0; j < m; ++j) {
@@ -197,7 +198,7 @@ void rand_rounding_general(ttc_context* c, int m, const double* alpha, const ttc
     for (int j = op ? 1 : 0; j < m; ++j) tt_terms.push_back(j);
     if (!tt_terms.empty()) {
       std::vector<std::vector<double*>> Wt;
-      if (sk.precision == TTC_PREC_BF16) emit_sketch_bf16(B, X, tt_terms, sp, S, Wt);
+      if (tensor_core_sketch(sk.precision)) emit_sketch_bf16(B, X, tt_terms, sp, S, Wt, sk.precision == TTC_PREC_TF32);
       else emit_sketch_f64(B, X, tt_terms, sp, S, Wt);
       for (size_t i = 0; i < tt_terms.size(); ++i) W[tt_terms[i]] = Wt[i];
     }

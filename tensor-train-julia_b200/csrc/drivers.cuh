@@ -28,8 +28,16 @@ void emit_sketch_blocks(Builder& B, const std::vector<long long>& dims, const Sk
                         const std::vector<const double*>& host_raw, std::vector<double*>& S);
 void emit_sketch_f64(Builder& B, ttc_batch* x, const std::vector<int>& tts, const SketchPlan& sp,
                      const std::vector<double*>& S, std::vector<std::vector<double*>>& W);
+// Sketch contractions on the tcgen05 tensor cores: BF16 operands, or FP32 operands read as
+// TF32 (tf32 = true); FP32 accumulation either way.
 void emit_sketch_bf16(Builder& B, ttc_batch* x, const std::vector<int>& tts, const SketchPlan& sp,
-                      const std::vector<double*>& S, std::vector<std::vector<double*>>& W);
+                      const std::vector<double*>& S, std::vector<std::vector<double*>>& W, bool tf32 = false);
+// Rejects a sketch precision other than TTC_PREC_FP64, TTC_PREC_BF16 and TTC_PREC_TF32.
+inline void check_precision(int p) {
+  TTC_REQUIRE(p == TTC_PREC_FP64 || p == TTC_PREC_BF16 || p == TTC_PREC_TF32, TTC_EARG,
+              "sketch precision must be TTC_PREC_FP64, TTC_PREC_BF16 or TTC_PREC_TF32");
+}
+inline bool tensor_core_sketch(int p) { return p == TTC_PREC_BF16 || p == TTC_PREC_TF32; }
 void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<int>& tts, const SketchPlan& sp,
                      const std::vector<std::vector<double*>>& W, const std::vector<std::vector<int>>& rho);
 std::vector<int> orth_left_ranks(const ttc_batch* x, int t);

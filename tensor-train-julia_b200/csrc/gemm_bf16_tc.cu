@@ -1,14 +1,16 @@
-// Grouped BF16 GEMM on the 5th-generation tensor cores (tcgen05, sm_100a), FP32
+// Grouped BF16 or TF32 GEMM on the 5th-generation tensor cores (tcgen05, sm_100a), FP32
 // accumulation in tensor memory.  Used for the reverse-sketch contractions of
 // tt_recursive_sketch (src/sketches.jl:1602-1638) in the mixed-precision rounding:
-//   C(i, j) = alpha * sum_k A(i, k) * B(j, k),   A and B K-major BF16 (row stride lda/ldb,
-//   a multiple of 8 elements, K zero padded to a multiple of 8).
-// Tile 128 x 128 x 64, one CTA (4 warps) per output tile.  Operand tiles are staged with
-// cp.async into the 128-byte-swizzled K-major layout that the UMMA shared-memory
-// descriptors describe; one elected thread issues tcgen05.mma (M=128, N=128, K=16) and
-// tcgen05.commit arrives on an mbarrier; a two-stage ring overlaps the next tile's loads
-// with the current MMAs.  The epilogue reads the accumulator with tcgen05.ld (32x32b)
-// and writes FP64 / FP32 / BF16 outputs with arbitrary (split) strides.
+//   C(i, j) = alpha * sum_k A(i, k) * B(j, k),   A and B K-major, BF16 (kind::f16) or FP32
+//   read as TF32 (kind::tf32), row stride lda/ldb a multiple of 8 (BF16) or 4 (FP32)
+//   elements, K zero padded to that multiple.
+// Tile 128 x 128 x (128 bytes of K: 64 BF16 or 32 FP32), one CTA (4 warps) per output tile.
+// Operand tiles are staged with cp.async into the 128-byte-swizzled K-major layout that the
+// UMMA shared-memory descriptors describe; one elected thread issues four tcgen05.mma per
+// tile (M=128, N=128, K=16 BF16 or K=8 TF32: 32 bytes of K each) and tcgen05.commit arrives
+// on an mbarrier; a two-stage ring overlaps the next tile's loads with the current MMAs.  The
+// epilogue reads the accumulator with tcgen05.ld (32x32b) and writes FP64 / FP32 outputs and
+// an operand-typed (BF16 or FP32) output with arbitrary (split) strides.
 // Every mbarrier wait is bounded: on timeout the kernel raises DFLAG_TIMEOUT, frees its
 // tensor memory and returns.
 #include <cuda_bf16.h>
@@ -17,8 +19,8 @@
 
 namespace ttc {
 namespace {
-constexpr int BM = 128, BN = 128, BK = 64, NT = 128, STAGES = 2;
-constexpr int TILE_BYTES = BM * BK * 2;                 // 16 KB per operand tile
+constexpr int BM = 128, BN = 128, NT = 128, STAGES = 2;
+constexpr int TILE_BYTES = BM * 128;                    // 16 KB per operand tile (128 B of K per row)
 constexpr uint32_t TMEM_COLS = 128;
 constexpr long long WAIT_LIMIT = 1LL << 24;             // bounded mbarrier polls
 
@@ -66,16 +68,31 @@ __device__ __forceinline__ uint64_t make_sdesc(uint32_t saddr) {
   return d;
 }
 
-// Instruction descriptor, kind::f16: D=F32, A=B=BF16, both K-major, M=128, N=128.
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// Instruction descriptor: D=F32 (bits 4-5), A and B format (bits 7-9, 10-12: 1 = BF16 for
+// kind::f16, 2 = TF32 for kind::tf32; A and B always the same type), both K-major, N>>3 at bit
+// 17, M>>4 at bit 24.
+template <bool TF32>
+__host__ __device__ constexpr uint32_t idesc() {
+  return (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)(BM >> 4) << 24);
+}
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate)
-      : "memory");
+template <bool TF32>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  if constexpr (TF32)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc<true>()), "r"(accumulate)
+        : "memory");
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc<false>()), "r"(accumulate)
+        : "memory");
 }
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar) : "memory");
@@ -105,7 +122,11 @@ __device__ __forceinline__ int find_desc(const Bf16GemmDesc* __restrict__ d, int
 }
 }  // namespace
 
+template <bool TF32>
 __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc* __restrict__ descs, int nd, int* flags) {
+  constexpr int EB = TF32 ? 4 : 2;         // operand element bytes
+  constexpr int BK = 128 / EB;             // K elements per 128-byte tile row
+  constexpr int CH = 16 / EB;              // K elements per 16-byte chunk
   extern __shared__ __align__(1024) unsigned char dsm[];
   __shared__ uint64_t mbar[STAGES];
   __shared__ uint32_t tmem_base_sh;
@@ -139,8 +160,8 @@ __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc*
   tc_fence_after();
   const uint32_t tmem = tmem_base_sh;
 
-  const __nv_bfloat16* Ag = reinterpret_cast<const __nv_bfloat16*>(D.A);
-  const __nv_bfloat16* Bg = reinterpret_cast<const __nv_bfloat16*>(D.B);
+  const char* Ag = reinterpret_cast<const char*>(D.A);
+  const char* Bg = reinterpret_cast<const char*>(D.B);
 
   // Each thread moves 8 of the 1024 16-byte chunks of each operand tile.
   auto load_stage = [&](int kt, int s) {
@@ -150,13 +171,13 @@ __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc*
     for (int t = 0; t < 8; ++t) {
       const int idx = tid + NT * t;          // 0..1023
       const int r = idx >> 3, c = idx & 7;   // row, 16-byte chunk within the 128-byte row
-      const int kk = k0 + c * 8;
+      const int kk = k0 + c * CH;
       const uint32_t off = (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
       const int gi = row0 + r, gj = col0 + r;
       const bool va = (gi < D.m) && (kk < D.k);
       const bool vb = (gj < D.n) && (kk < D.k);
-      cp_async_16(sa + off, va ? (const void*)(Ag + (long long)gi * D.lda + kk) : (const void*)Ag, va);
-      cp_async_16(sb + off, vb ? (const void*)(Bg + (long long)gj * D.ldb + kk) : (const void*)Bg, vb);
+      cp_async_16(sa + off, va ? (const void*)(Ag + ((long long)gi * D.lda + kk) * EB) : (const void*)Ag, va);
+      cp_async_16(sb + off, vb ? (const void*)(Bg + ((long long)gj * D.ldb + kk) * EB) : (const void*)Bg, vb);
     }
     cp_async_commit();
   };
@@ -179,8 +200,8 @@ __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc*
       tc_fence_after();
       const uint32_t sa = smem_u32(As + s * TILE_BYTES), sb = smem_u32(Bs + s * TILE_BYTES);
 #pragma unroll
-      for (int kk = 0; kk < BK / 16; ++kk) {
-        umma_bf16(tmem, make_sdesc(sa + kk * 32), make_sdesc(sb + kk * 32), (kt > 0 || kk > 0) ? 1u : 0u);
+      for (int kk = 0; kk < 4; ++kk) {   // 32 bytes of K per MMA
+        umma<TF32>(tmem, make_sdesc(sa + kk * 32), make_sdesc(sb + kk * 32), (kt > 0 || kk > 0) ? 1u : 0u);
       }
       umma_commit(smem_u32(&mbar[s]));
     }
@@ -212,7 +233,10 @@ __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc*
             const double x = D.alpha * (double)v[i];
             if (D.C64) D.C64[roff64 + (long long)col * D.c_j] = x;
             if (D.C32) reinterpret_cast<float*>(D.C32)[roff64 + (long long)col * D.c_j] = (float)x;
-            if (D.C16) reinterpret_cast<__nv_bfloat16*>(D.C16)[roff16 + (long long)col * D.h_j] = __double2bfloat16(x);
+            if (D.C16) {   // operand-typed output
+              if constexpr (TF32) reinterpret_cast<float*>(D.C16)[roff16 + (long long)col * D.h_j] = round_tf32((float)x);
+              else reinterpret_cast<__nv_bfloat16*>(D.C16)[roff16 + (long long)col * D.h_j] = __double2bfloat16(x);
+            }
           }
         }
       }
@@ -230,16 +254,27 @@ long long bf16_gemm_tiles(const Bf16GemmDesc& d) {
   return (long long)((d.m + BM - 1) / BM) * ((d.n + BN - 1) / BN);
 }
 
-void launch_gemm_bf16_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags) {
-  if (nd <= 0 || total_tiles <= 0) return;
+namespace {
+template <bool TF32>
+void launch_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags) {
   const int smem = STAGES * 2 * TILE_BYTES + 1024;
-  static bool attr = false;
-  if (!attr) {
-    TTC_CUDA(cudaFuncSetAttribute(gemm_bf16_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr = true;
+  static int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    TTC_CUDA(cudaFuncSetAttribute(gemm_bf16_tc_kernel<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr_dev = dev;
   }
-  gemm_bf16_tc_kernel<<<(unsigned)total_tiles, NT, smem, s>>>(d, nd, d_flags);
+  gemm_bf16_tc_kernel<TF32><<<(unsigned)total_tiles, NT, smem, s>>>(d, nd, d_flags);
   TTC_CHECK_LAUNCH();
+}
+}  // namespace
+
+void launch_gemm_bf16_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags,
+                         bool tf32) {
+  if (nd <= 0 || total_tiles <= 0) return;
+  if (tf32) launch_tc<true>(d, nd, total_tiles, s, d_flags);
+  else launch_tc<false>(d, nd, total_tiles, s, d_flags);
 }
 
 }  // namespace ttc

@@ -54,6 +54,7 @@ void rand_rounding_host(ttc_context* c, int m, const double* alpha, const ttc_tt
   const SketchPlan sp = sketch_plan(xb->dims, r, sk.block_rks);
   const std::vector<int> cap = rand_out_ranks(xb->dims, sp);
   ttc_batch* yb = H.add(batch_create(c, 1, N, xb->dims.data(), cap.data()));
+  check_precision(sk.precision);
   std::string key;
   const auto raw = upload_host_blocks(c, xb->dims, sp, sk.sketch_blocks, key);
   round_rand(c, xb, r, sk, after, yb, raw, key);
@@ -84,6 +85,7 @@ void recursive_sketch_host(ttc_context* c, const ttc_ttv* Ah, const ttc_tto* Hh,
     TTC_REQUIRE(H->N == N && H->dims == xb->dims, TTC_EDIM, "tt_recursive_sketch: operator and TT dims differ");
     TTC_REQUIRE(H->rks[N] == 1, TTC_EDIM, "tt_recursive_sketch: last operator rank must be 1");
   }
+  check_precision(sk.precision);
   std::string key;
   const auto raw = upload_host_blocks(c, xb->dims, sp, sk.sketch_blocks, key);
   // output sizes
@@ -109,7 +111,7 @@ void recursive_sketch_host(ttc_context* c, const ttc_ttv* Ah, const ttc_tto* Hh,
       emit_sketch_op_f64(B, *H, xb, 0, sp, S, Wk);
     } else {
       std::vector<std::vector<double*>> W;
-      if (sk.precision == TTC_PREC_BF16) emit_sketch_bf16(B, xb, {0}, sp, S, W);
+      if (tensor_core_sketch(sk.precision)) emit_sketch_bf16(B, xb, {0}, sp, S, W, sk.precision == TTC_PREC_TF32);
       else emit_sketch_f64(B, xb, {0}, sp, S, W);
       Wk = W[0];
     }

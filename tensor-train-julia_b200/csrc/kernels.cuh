@@ -122,17 +122,19 @@ struct PhiloxDesc { double* dst; long long count; unsigned long long seed; unsig
 void launch_philox(const PhiloxDesc* d, int count, long long max_count, cudaStream_t s);
 
 // ---- FP64 -> BF16 conversion and the tcgen05 BF16 GEMM (gemm_bf16_tc.cu)
+// Operands are BF16, or FP32 read as TF32 in a launch with tf32 = true.
 struct Bf16GemmDesc {
   int m, n, k, m0;                // m0: row split (row i = i0 + m0*i1) of the outputs
-  const void* A; long long lda;   // bf16, K-major: A(i, kk) at A[i*lda + kk]
-  const void* B; long long ldb;   // bf16, K-major: B(j, kk) at B[j*ldb + kk]
+  const void* A; long long lda;   // operand type, K-major: A(i, kk) at A[i*lda + kk]
+  const void* B; long long ldb;   // operand type, K-major: B(j, kk) at B[j*ldb + kk]
   double* C64; float* C32;        // outputs sharing strides: (i0*c_i0 + i1*c_i1 + j*c_j)
-  void* C16;                      // bf16 output with strides (h_i0, h_i1, h_j)
+  void* C16;                      // output in the operand type (BF16 or FP32), strides (h_i0, h_i1, h_j)
   long long c_i0, c_i1, c_j, h_i0, h_i1, h_j;
   double alpha;
   long long tile_start;
 };
-void launch_gemm_bf16_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags);
+void launch_gemm_bf16_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags,
+                         bool tf32 = false);
 long long bf16_gemm_tiles(const Bf16GemmDesc& d);
 
 }  // namespace ttc

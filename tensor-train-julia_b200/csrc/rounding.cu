@@ -481,6 +481,7 @@ void round_rand(ttc_context* c, ttc_batch* x, const std::vector<long long>& rks,
                 const std::string& raw_key) {
   TTC_REQUIRE(x != y, TTC_EARG, "round: input and output batches must differ");
   TTC_REQUIRE(y->count == x->count && y->N == x->N && y->dims == x->dims, TTC_EDIM, "round: output batch shape differs");
+  check_precision(o.precision);
   const int N = x->N;
   TTC_REQUIRE((int)rks.size() == N + 1, TTC_EDIM, "ttrand_rounding: rks must have length N+1");
   TTC_REQUIRE(rks[N] == 1, TTC_EDIM, "ttrand_rounding: rks[N+1] must be 1");
@@ -513,7 +514,7 @@ void round_rand(ttc_context* c, ttc_batch* x, const std::vector<long long>& rks,
     std::vector<double*> S;
     emit_sketch_blocks(B, x->dims, sp, o, host_raw, S);
     std::vector<std::vector<double*>> W;
-    if (o.precision == TTC_PREC_BF16) emit_sketch_bf16(B, x, all, sp, S, W);
+    if (tensor_core_sketch(o.precision)) emit_sketch_bf16(B, x, all, sp, S, W, o.precision == TTC_PREC_TF32);
     else emit_sketch_f64(B, x, all, sp, S, W);
     B.stage(1);
     emit_rand_sweep(B, x, y, all, sp, W, rho_all);

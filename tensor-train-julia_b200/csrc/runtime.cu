@@ -46,19 +46,23 @@ void launch_setrank(const SetRankDesc* d, int count, cudaStream_t s) {
   TTC_CHECK_LAUNCH();
 }
 
+template <typename T>
 __global__ void cvt_bf16_kernel(const CvtDesc* descs) {
   const CvtDesc D = descs[blockIdx.y];
   const long long total = D.rows * D.cols;
-  __nv_bfloat16* dst = reinterpret_cast<__nv_bfloat16*>(D.dst);
+  T* dst = reinterpret_cast<T*>(D.dst);
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
     const long long i = e % D.rows, j = e / D.rows;
-    dst[i * D.ds_i + j * D.ds_j] = __double2bfloat16(D.alpha * D.src[i * D.ss_i + j * D.ss_j]);
+    const double v = D.alpha * D.src[i * D.ss_i + j * D.ss_j];
+    if constexpr (sizeof(T) == 4) dst[i * D.ds_i + j * D.ds_j] = round_tf32((float)v);   // TF32 operand
+    else dst[i * D.ds_i + j * D.ds_j] = __double2bfloat16(v);
   }
 }
-void launch_cvt_bf16(const CvtDesc* d, int count, long long max_elems, cudaStream_t s) {
+void launch_cvt_bf16(const CvtDesc* d, int count, long long max_elems, cudaStream_t s, bool f32) {
   if (count <= 0 || max_elems <= 0) return;
   const long long blocks = std::min<long long>((max_elems + 255) / 256, 148LL * 8);
-  cvt_bf16_kernel<<<dim3((unsigned)blocks, (unsigned)count), 256, 0, s>>>(d);
+  if (f32) cvt_bf16_kernel<float><<<dim3((unsigned)blocks, (unsigned)count), 256, 0, s>>>(d);
+  else cvt_bf16_kernel<__nv_bfloat16><<<dim3((unsigned)blocks, (unsigned)count), 256, 0, s>>>(d);
   TTC_CHECK_LAUNCH();
 }
 
@@ -93,11 +97,11 @@ static void launch_op(ttc_context* c, const Plan& p, const Op& op) {
       case OP_SUMSQ: launch_sumsq((const NormDesc*)d, op.count, s); break;
       case OP_APPLY: launch_apply((const ApplyDesc*)d, op.count, op.total, s); break;
       case OP_PHILOX: launch_philox((const PhiloxDesc*)d, op.count, op.total, s); break;
-      case OP_BF16GEMM: launch_gemm_bf16_tc((const Bf16GemmDesc*)d, op.count, op.total, s, c->d_flags); break;
+      case OP_BF16GEMM: launch_gemm_bf16_tc((const Bf16GemmDesc*)d, op.count, op.total, s, c->d_flags, op.a != 0); break;
       case OP_ZEROCHK: launch_zerochk((const ZeroChkDesc*)d, op.count, s); break;
       case OP_FINAL: launch_final((const FinalDesc*)d, op.count, op.total, s); break;
       case OP_SETRANK: launch_setrank((const SetRankDesc*)d, op.count, s); break;
-      case OP_CVT_BF16: launch_cvt_bf16((const CvtDesc*)d, op.count, op.total, s); break;
+      case OP_CVT_BF16: launch_cvt_bf16((const CvtDesc*)d, op.count, op.total, s, op.a != 0); break;
       case OP_STAGE: TTC_CUDA(cudaEventRecord(c->ev[op.a], s)); break;
     }
   }
@@ -494,19 +498,20 @@ void Builder::philox(const std::vector<PhiloxDesc>& v) {
   Op op; op.kind = OP_PHILOX; op.off = plan->push(v); op.count = (int)v.size(); op.total = mx;
   plan->ops.push_back(op);
 }
-void Builder::bf16gemm(std::vector<Bf16GemmDesc> v) {
+void Builder::bf16gemm(std::vector<Bf16GemmDesc> v, bool tf32) {
   std::vector<Bf16GemmDesc> w;
   long long t = 0;
+  const long long esz = tf32 ? 4 : 2, chunk = 16 / esz;   // operand bytes, elements per 16 bytes
   for (auto& d : v) {
     const long long n = bf16_gemm_tiles(d);
     if (n == 0) continue;
     if (wsbase) {
-      TTC_REQUIRE(d.lda % 8 == 0 && d.ldb % 8 == 0 && d.lda >= d.k && d.ldb >= d.k && d.m0 >= 1, TTC_EINTERNAL,
-                  "bf16 gemm: leading dims must be multiples of 8 covering K");
+      TTC_REQUIRE(d.lda % chunk == 0 && d.ldb % chunk == 0 && d.lda >= d.k && d.ldb >= d.k && d.m0 >= 1,
+                  TTC_EINTERNAL, "tensor-core gemm: leading dims must be multiples of 16 bytes covering K");
       TTC_REQUIRE(((uintptr_t)d.A % 16) == 0 && ((uintptr_t)d.B % 16) == 0, TTC_EINTERNAL, "bf16 gemm: 16-byte alignment");
-      const long long kp = (d.k + 7) / 8 * 8;
-      region_check(d.A, 2 * (size_t)(d.lda * (d.m - 1) + kp), "bf16 A");
-      region_check(d.B, 2 * (size_t)(d.ldb * (d.n - 1) + kp), "bf16 B");
+      const long long kp = (d.k + chunk - 1) / chunk * chunk;
+      region_check(d.A, esz * (size_t)(d.lda * (d.m - 1) + kp), "bf16 A");
+      region_check(d.B, esz * (size_t)(d.ldb * (d.n - 1) + kp), "bf16 B");
       const long long mi0 = std::min(d.m, d.m0), mi1 = (d.m - 1) / d.m0 + 1;
       if (d.C64 || d.C32) {
         const long long e[3] = {mi0, mi1, d.n}, s[3] = {d.c_i0, d.c_i1, d.c_j};
@@ -515,7 +520,7 @@ void Builder::bf16gemm(std::vector<Bf16GemmDesc> v) {
       }
       if (d.C16) {
         const long long e[3] = {mi0, mi1, d.n}, s[3] = {d.h_i0, d.h_i1, d.h_j};
-        region_check(d.C16, 2 * (size_t)span_elems(e, s, 3), "bf16 C16");
+        region_check(d.C16, esz * (size_t)span_elems(e, s, 3), "bf16 C16");
       }
     }
     d.tile_start = t;
@@ -523,21 +528,21 @@ void Builder::bf16gemm(std::vector<Bf16GemmDesc> v) {
     w.push_back(d);
   }
   if (w.empty()) return;
-  Op op; op.kind = OP_BF16GEMM; op.off = plan->push(w); op.count = (int)w.size(); op.total = t;
+  Op op; op.kind = OP_BF16GEMM; op.off = plan->push(w); op.count = (int)w.size(); op.total = t; op.a = tf32;
   for (auto& d : w) op.flops += 2.0 * d.m * d.n * d.k;
   plan->ops.push_back(op);
 }
-void Builder::cvt_bf16(const std::vector<CvtDesc>& v) {
+void Builder::cvt_bf16(const std::vector<CvtDesc>& v, bool f32) {
   if (v.empty()) return;
   long long mx = 0;
   for (auto& d : v) {
     mx = std::max(mx, d.rows * d.cols);
     if (wsbase) {
       region_check(d.src, 8 * (size_t)sp2(d.rows, d.ss_i, d.cols, d.ss_j), "cvt src");
-      region_check(d.dst, 2 * (size_t)sp2(d.rows, d.ds_i, d.cols, d.ds_j), "cvt dst");
+      region_check(d.dst, (f32 ? 4 : 2) * (size_t)sp2(d.rows, d.ds_i, d.cols, d.ds_j), "cvt dst");
     }
   }
-  Op op; op.kind = OP_CVT_BF16; op.off = plan->push(v); op.count = (int)v.size(); op.total = mx;
+  Op op; op.kind = OP_CVT_BF16; op.off = plan->push(v); op.count = (int)v.size(); op.total = mx; op.a = f32;
   plan->ops.push_back(op);
 }
 void Builder::zerochk(const std::vector<ZeroChkDesc>& v) {

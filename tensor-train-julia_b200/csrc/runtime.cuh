@@ -53,7 +53,8 @@ struct CvtDesc { const double* src; void* dst; long long rows, cols, ss_i, ss_j,
 void launch_zerochk(const ZeroChkDesc* d, int count, cudaStream_t s);
 void launch_final(const FinalDesc* d, int count, long long max_n, cudaStream_t s);
 void launch_setrank(const SetRankDesc* d, int count, cudaStream_t s);
-void launch_cvt_bf16(const CvtDesc* d, int count, long long max_elems, cudaStream_t s);
+// FP64 -> BF16 (f32 = false) or FP64 -> FP32 rounded to TF32 (f32 = true), same index map.
+void launch_cvt_bf16(const CvtDesc* d, int count, long long max_elems, cudaStream_t s, bool f32 = false);
 
 struct Plan {
   std::vector<unsigned char> blob;

@@ -26,14 +26,16 @@ namespace ttc {
 static inline long long pad8(long long v) { return (v + 7) & ~7LL; }
 
 void emit_sketch_bf16(Builder& B, ttc_batch* x, const std::vector<int>& tts, const SketchPlan& sp,
-                      const std::vector<double*>& S, std::vector<std::vector<double*>>& W) {
+                      const std::vector<double*>& S, std::vector<std::vector<double*>>& W, bool tf32) {
   const int N = x->N;
   const size_t T = tts.size();
   W.assign(T, std::vector<double*>(N + 1, nullptr));
-  // BF16 buffers are carved from double-sized workspace blocks (zeroed: padding must be 0).
+  const long long esz = tf32 ? 4 : 2;   // operand bytes: BF16, or FP32 read as TF32
+  auto at = [&](const void* p, long long elems) -> void* { return (void*)((const char*)p + elems * esz); };
+  // Operand buffers are carved from double-sized workspace blocks (zeroed: padding must be 0).
   std::vector<ZeroDesc> zr;
   auto bf = [&](long long elems) -> void* {
-    const long long nd = (elems + 3) / 4;
+    const long long nd = (elems * esz + 7) / 8;
     double* p = B.wd((size_t)nd);
     zr.push_back({p, nd});
     return (void*)p;
@@ -62,7 +64,7 @@ void emit_sketch_bf16(Builder& B, ttc_batch* x, const std::vector<int>& tts, con
       for (long long z = 0; z < n; ++z) {
         CvtDesc c{};
         c.src = x->core(t, k) + z * xc;
-        c.dst = (void*)((unsigned short*)A16[i][k] + r0 * z * lda);
+        c.dst = at(A16[i][k], r0 * z * lda);
         c.rows = r0; c.cols = r1;
         c.ss_i = 1; c.ss_j = xc * n;
         c.ds_i = lda; c.ds_j = 1;
@@ -84,7 +86,7 @@ void emit_sketch_bf16(Builder& B, ttc_batch* x, const std::vector<int>& tts, con
     for (long long j = 0; j < pk; ++j) {
       CvtDesc c{};
       c.src = S[k] + j * n * bl * br;
-      c.dst = (void*)((unsigned short*)S16[k] + j * lds * br);
+      c.dst = at(S16[k], j * lds * br);
       c.rows = n * bl; c.cols = br;
       c.ss_i = 1; c.ss_j = n * bl;
       c.ds_i = 1; c.ds_j = lds;
@@ -93,7 +95,7 @@ void emit_sketch_bf16(Builder& B, ttc_batch* x, const std::vector<int>& tts, con
     }
   }
   B.zero(zr);
-  B.cvt_bf16(cv);
+  B.cvt_bf16(cv, tf32);
   for (int k = N - 1; k >= 0; --k) {
     const size_t mk = B.mark();
     std::vector<ZeroDesc> zt;
@@ -135,35 +137,35 @@ void emit_sketch_bf16(Builder& B, ttc_batch* x, const std::vector<int>& tts, con
         }
         continue;
       }
-      const long long tnd = (r0 * ldt * pk + 3) / 4;
+      const long long tnd = (r0 * ldt * pk * esz + 7) / 8;
       double* Tbuf = B.wd((size_t)tnd);
       zt.push_back({Tbuf, tnd});
       for (long long j = 0; j < pk; ++j) {
-        unsigned short* T16 = (unsigned short*)Tbuf + j * r0 * ldt;
+        void* T16 = at(Tbuf, j * r0 * ldt);
         Bf16GemmDesc d{};
         d.m = (int)(r0 * n); d.n = (int)bl; d.k = (int)r1; d.m0 = (int)r0;
         d.A = A16[i][k]; d.lda = ldw1;
         const long long jn = (k < N - 1) ? j : 0;
-        d.B = (const void*)((const unsigned short*)W16[i][k + 1] + jn * ldw1 * bl); d.ldb = ldw1;
+        d.B = at(W16[i][k + 1], jn * ldw1 * bl); d.ldb = ldw1;
         d.C16 = T16; d.h_i0 = ldt; d.h_i1 = 1; d.h_j = n;
         d.alpha = 1.0;
         g1.push_back(d);
         Bf16GemmDesc e{};
         e.m = (int)r0; e.n = (int)br; e.k = (int)(n * bl); e.m0 = (int)std::max<long long>(r0, 1);
         e.A = T16; e.lda = ldt;
-        e.B = (const void*)((const unsigned short*)S16[k] + j * lds * br); e.ldb = lds;
+        e.B = at(S16[k], j * lds * br); e.ldb = lds;
         e.C64 = W[i][k] + j * r0 * br; e.c_i0 = 1; e.c_i1 = 0; e.c_j = r0;
-        if (k > 0) { e.C16 = (unsigned short*)W16[i][k] + j * ldw0 * br; e.h_i0 = 1; e.h_i1 = 0; e.h_j = ldw0; }
+        if (k > 0) { e.C16 = at(W16[i][k], j * ldw0 * br); e.h_i0 = 1; e.h_i1 = 0; e.h_j = ldw0; }
         e.alpha = 1.0;
         g2.push_back(e);
       }
     }
     B.zero(zt);
-    B.bf16gemm(g1);
-    B.bf16gemm(g2);
+    B.bf16gemm(g1, tf32);
+    B.bf16gemm(g2, tf32);
     B.gemm(f1);
     B.gemm(f2);
-    B.cvt_bf16(cw);
+    B.cvt_bf16(cw, tf32);
     B.release(mk);
   }
 }

@@ -133,4 +133,31 @@ int ttc_test_bf16_gemm(ttc_context* c, int m, int n, int k, const double* A, con
   });
 }
 
+// tcgen05 TF32 GEMM: as ttc_test_bf16_gemm with the operands converted to FP32 and read by the
+// tensor cores as TF32 (kind::tf32).
+int ttc_test_tf32_gemm(ttc_context* c, int m, int n, int k, const double* A, const double* Bh, double* C,
+                       double alpha) {
+  return hook(c, [&] {
+    const long long lda = (k + 3) / 4 * 4;
+    DevBuf dA((size_t)m * k * 8), dB((size_t)n * k * 8), dC((size_t)m * n * 8);
+    DevBuf a32((size_t)m * lda * 4 + 64), b32((size_t)n * lda * 4 + 64);
+    TTC_CUDA(cudaMemcpy(dA.p, A, (size_t)m * k * 8, cudaMemcpyHostToDevice));
+    TTC_CUDA(cudaMemcpy(dB.p, Bh, (size_t)n * k * 8, cudaMemcpyHostToDevice));
+    TTC_CUDA(cudaMemset(a32.p, 0, (size_t)m * lda * 4 + 64));
+    TTC_CUDA(cudaMemset(b32.p, 0, (size_t)n * lda * 4 + 64));
+    run_plan_once(c, [&](Builder& B) {
+      CvtDesc ca{dA.as<double>(), a32.p, m, k, k, 1, lda, 1, 1.0};
+      CvtDesc cb{dB.as<double>(), b32.p, n, k, k, 1, lda, 1, 1.0};
+      B.cvt_bf16({ca, cb}, true);
+      Bf16GemmDesc d{};
+      d.m = m; d.n = n; d.k = k; d.m0 = std::max(m, 1);
+      d.A = a32.p; d.lda = lda; d.B = b32.p; d.ldb = lda;
+      d.C64 = dC.as<double>(); d.c_i0 = 1; d.c_i1 = 0; d.c_j = m;
+      d.alpha = alpha;
+      B.bf16gemm({d}, true);
+    });
+    TTC_CUDA(cudaMemcpy(C, dC.p, (size_t)m * n * 8, cudaMemcpyDeviceToHost));
+  });
+}
+
 }  // extern "C"

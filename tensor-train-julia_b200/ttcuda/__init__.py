@@ -291,7 +291,9 @@ class _Out:
 
 
 def _sketch_opts(orthogonal, seed, block_rks, precision, sketch_blocks, keep) -> L.SketchOpts:
-    prec = {"fp64": 0, "bf16": 1, 0: 0, 1: 1}[precision]
+    prec = {"fp64": 0, "bf16": 1, "tf32": 2, 0: 0, 1: 1, 2: 2}.get(precision)
+    if prec is None:
+        raise ArgumentError(f"precision must be 'fp64', 'bf16' or 'tf32', not {precision!r}")
     sb = None
     if sketch_blocks is not None:
         sb = _ptrs([np.asfortranarray(b, dtype=np.float64) for b in sketch_blocks], keep)

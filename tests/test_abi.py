@@ -69,3 +69,13 @@ def test_no_gpu_calls_fail_cleanly_without_device(built_lib):
         pytest.skip("a GPU is present")
     with pytest.raises(Exception):
         ttcuda.Context(0)
+
+
+def test_sketch_precision_names(built_lib):
+    """precision is 'fp64', 'bf16' or 'tf32' (TTC_PREC_FP64/_BF16/_TF32); anything else is an
+    ArgumentError before any device work."""
+    import ttcuda
+    keep = ttcuda._Keep()
+    assert [ttcuda._sketch_opts(True, 1, None, p, None, keep).precision for p in ("fp64", "bf16", "tf32")] == [0, 1, 2]
+    with pytest.raises(ttcuda.ArgumentError):
+        ttcuda._sketch_opts(True, 1, None, "fp16", None, keep)

@@ -17,6 +17,7 @@ lib.ttc_test_gemm.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.
 lib.ttc_test_qr.argtypes = [C.c_void_p, C.c_int, C.c_int, P, P, P]
 lib.ttc_test_jacobi.argtypes = [C.c_void_p, C.c_int, C.c_int, P, C.c_int, P, P, PI, PI]
 lib.ttc_test_bf16_gemm.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, P, P, P, C.c_double]
+lib.ttc_test_tf32_gemm.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, P, P, P, C.c_double]
 
 
 def ptr(a):
@@ -163,3 +164,23 @@ def test_bf16_tcgen05_gemm(ctx, m, n, k):
     worst = np.unravel_index(np.argmax(ratio), ratio.shape)
     assert ratio.max() <= 1.0, f"worst element {worst}: got {got[worst]}, ref {ref[worst]}, bound {bound[worst]}"
     assert np.linalg.norm(got - ref) <= 1e-6 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (128, 128, 32), (200, 130, 100), (513, 257, 266), (40, 300, 4)])
+def test_tf32_tcgen05_gemm(ctx, m, n, k):
+    """kind::tf32: FP32 operands read with a 10-bit mantissa (each operand's relative error
+    below 2^-10, so a product's below 2^-9), FP32 accumulation."""
+    g = np.random.default_rng(m + 5 * n + 11 * k)
+    A = g.standard_normal((m, k))
+    B = g.standard_normal((n, k))
+    Cm = np.zeros(m * n)
+    ctx.check(lib.ttc_test_tf32_gemm(ctx.h, m, n, k, ptr(np.ascontiguousarray(A)), ptr(np.ascontiguousarray(B)),
+                                     ptr(Cm), 1.0))
+    ref = A @ B.T
+    got = Cm.reshape((m, n), order="F")
+    mag = np.abs(A) @ np.abs(B).T
+    bound = (2.0 ** -9 + 4 * np.sqrt(k) * 2.0 ** -24) * mag
+    ratio = np.abs(got - ref) / (bound + 1e-30)
+    worst = np.unravel_index(np.argmax(ratio), ratio.shape)
+    assert ratio.max() <= 1.0, f"worst element {worst}: got {got[worst]}, ref {ref[worst]}, bound {bound[worst]}"
+    assert np.linalg.norm(got - ref) <= 2e-3 * np.linalg.norm(ref)

@@ -189,6 +189,30 @@ def test_ttrand_rounding_device_sketch_and_default_heuristic():
     assert rel(got, x) < 1e-11     # sketch rank covers the TT rank: exact up to rounding
 
 
+def test_recursive_sketch_tf32_closer_than_bf16():
+    """TF32 sketch contractions (FP32 operands, 10-bit mantissa on the tensor cores) track the
+    FP64 sketch more closely than BF16 (7-bit)."""
+    x = o.rand_tt((2,) * 10, 8, np.random.default_rng(13))
+    rks = o.default_rank_heuristic(x)
+    Wr, _ = o.tt_recursive_sketch(x, rks, orthogonal=False, seed=5, block_rks=32, rng_kind="philox")
+    Wt, _ = ttcuda.tt_recursive_sketch(to_dev(x), rks, orthogonal=False, seed=5, block_rks=32, precision="tf32")
+    Wb, _ = ttcuda.tt_recursive_sketch(to_dev(x), rks, orthogonal=False, seed=5, block_rks=32, precision="bf16")
+    et = sum(np.linalg.norm(a - b) ** 2 for a, b in zip(Wt, Wr)) ** 0.5
+    eb = sum(np.linalg.norm(a - b) ** 2 for a, b in zip(Wb, Wr)) ** 0.5
+    nr = sum(np.linalg.norm(b) ** 2 for b in Wr) ** 0.5
+    assert et <= 5e-3 * nr
+    assert et < eb
+
+
+def test_ttrand_rounding_tf32_sketch_accuracy():
+    """TF32 sketch, FP64 range finder and projection: s >= r keeps the TT to 1e-8."""
+    x = decaying_tt((2,) * 14, [1, 2, 4, 8, 16, 32, 32, 32, 32, 32, 16, 8, 4, 2, 1], seed=16)
+    rks = o.default_rank_heuristic(x)
+    got = ttcuda.ttrand_rounding(to_dev(x), rks, orthogonal=False, seed=3, block_rks=64, precision="tf32")
+    assert got.ttv_rks == o.ttrand_rounding(x, rks, orthogonal=False, seed=3, block_rks=64).ttv_rks
+    assert rel(got, x) < 1e-8
+
+
 def test_ttrand_rounding_bf16_sketch_accuracy():
     """Mixed precision: BF16 sketch, FP64 range finder/projection; s >= r keeps 1e-8."""
     x = decaying_tt((2,) * 14, [1, 2, 4, 8, 16, 32, 32, 32, 32, 32, 16, 8, 4, 2, 1], seed=16)
@@ -388,7 +412,7 @@ def test_batched_round_rand_then_svd():
     s = ttcuda._sketch_ranks(dims, rks, 64)
     cap = ttcuda._rand_out_caps(dims, s)
     yb = ttcuda.DeviceBatch(dims, [cap] * 3)
-    for prec in ("fp64", "bf16"):
+    for prec in ("fp64", "bf16", "tf32"):
         xb.round_rand(yb, rks, orthogonal=False, seed=4, block_rks=64, precision=prec, after_tol=1e-5)
         for t, got in zip(tts, yb.download()):
             ref = o.tt_rounding(o.ttrand_rounding(t, rks, orthogonal=False, seed=4, block_rks=64), tol=1e-5)
