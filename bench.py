@@ -234,6 +234,7 @@ def main():
     xb = ttcuda.DeviceBatch.from_tts(tt_objs, ctx=ctx)
     y_mixed = ttcuda.DeviceBatch(dims, [rho] * len(tts), ctx=ctx)
     y_fp64 = ttcuda.DeviceBatch(dims, ranks, ctx=ctx)
+    y_tf32 = ttcuda.DeviceBatch(dims, [rho] * len(tts), ctx=ctx)
 
     def step_mixed(sync=False):
         xb.round_rand(y_mixed, rks, orthogonal=True, seed=1234, block_rks=block, precision="bf16",
@@ -241,6 +242,10 @@ def main():
 
     def step_fp64(sync=False):
         xb.round_det(y_fp64, tol=TOL, sync=sync)
+
+    def step_tf32(sync=False):     # the same randomized rounding with TF32 sketch contractions
+        xb.round_rand(y_tf32, rks, orthogonal=True, seed=1234, block_rks=block, precision="tf32",
+                      after_tol=TOL, sync=sync)
 
     def barrier():
         torch.cuda.synchronize()
@@ -261,6 +266,7 @@ def main():
     for _ in range(max(3, args.warmup)):
         step_mixed(sync=True)
         step_fp64(sync=True)
+        step_tf32(sync=True)
     ctx.synchronize()
 
     # L2: the resident inputs (sum of core bytes) exceed the 126 MB L2
@@ -271,12 +277,15 @@ def main():
     with ClockSampler(clock_path) as cs:
         ms_mixed = timed(step_mixed, args.steps)
         ms_fp64 = timed(step_fp64, args.steps)
+        ms_tf32 = timed(step_tf32, args.steps)
+    launches_t = ctx.stats()["kernel_launches"]     # launches of one TF32 step (the last plan run)
     ctx.synchronize()
     clocks = cs.summary(local)
 
     nb = len(tts) * world
     value = shard.whole_job_rate(len(tts), world, args.steps, ms_mixed)
     fp64_value = shard.whole_job_rate(len(tts), world, args.steps, ms_fp64)
+    tf32_value = shard.whole_job_rate(len(tts), world, args.steps, ms_tf32)
 
     # accuracy on the GPU: ||x - round(x)|| / ||x|| through the library (difference TT, norm)
     def rel_err(x, y):
@@ -290,6 +299,9 @@ def main():
     err_fp64 = max(rel_err(tt_objs[i], out_f[i]) for i in range(nerr))
     err_mf = max(rel_err(out_f[i], out_m[i]) for i in range(nerr))
     ranks_equal = all(out_m[i].ttv_rks == out_f[i].ttv_rks for i in range(len(tts)))
+    out_t = y_tf32.download()
+    err_tf = max(rel_err(out_f[i], out_t[i]) for i in range(nerr))
+    ranks_equal_tf = all(out_t[i].ttv_rks == out_f[i].ttv_rks for i in range(len(tts)))
 
     # per-kernel profile of one extra step of each variant (event pair around every launch)
     ctx.set_profiling(True)
@@ -314,19 +326,27 @@ def main():
     launches_f, sw_f = st["kernel_launches"], sweeps(st)
     ctx.set_profiling(False)
 
-    # FP64 peak of this GPU (cuBLAS DGEMM, best of 5): the roofline denominator of the FP64 kernels
-    a = torch.randn(4096, 4096, dtype=torch.float64, device=f"cuda:{local}")
-    bmat = torch.randn(4096, 4096, dtype=torch.float64, device=f"cuda:{local}")
-    best = 1e9
-    for _ in range(5):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+    # FP64 and TF32 peaks of this GPU (torch.matmul, best of 10): the roofline denominators of
+    # the FP64 kernels and of the TF32 sketch
+    def matmul_peak(nmat, dtype):
+        a = torch.randn(nmat, nmat, dtype=dtype, device=f"cuda:{local}")
+        bmat = torch.randn(nmat, nmat, dtype=dtype, device=f"cuda:{local}")
         torch.matmul(a, bmat)
-        e1.record()
-        torch.cuda.synchronize()
-        best = min(best, e0.elapsed_time(e1))
-    fp64_peak_tflops = 2 * 4096 ** 3 / (best / 1e3) / 1e12
-    del a, bmat
+        best = 1e9
+        for _ in range(10):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, bmat)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return 2 * nmat ** 3 / (best / 1e3) / 1e12
+
+    fp64_peak_tflops = matmul_peak(4096, torch.float64)
+    allow = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    tf32_peak_tflops = matmul_peak(8192, torch.float32)
+    torch.backends.cuda.matmul.allow_tf32 = allow
 
     # dominant kernel of the mixed step: device time per launch (event pair around each launch)
     # and its algorithmic FLOPs per launch (the library's fixed conventions, from the launch shapes)
@@ -377,6 +397,12 @@ def main():
                        "l2": f"inputs {in_bytes / 1e6:.0f} MB resident > 126 MB L2"},
             "fp64": {"value": fp64_value, "unit": "roundings/s", "ms_per_step": ms_fp64 / args.steps,
                      "variant": "deterministic tt_rounding (FP64 Householder QR sweep + Jacobi SVD sweep)"},
+            "tf32": {"value": tf32_value, "unit": "roundings/s", "ms_per_step": ms_tf32 / args.steps,
+                     "variant": "TF32-sketch (tcgen05 kind::tf32) ttrand_rounding + FP64 SVD sweep",
+                     "rel_diff_vs_fp64": err_tf, "ranks_identical_fp64": ranks_equal_tf},
+            "peaks": {"fp64_tflops": fp64_peak_tflops, "tf32_tflops": tf32_peak_tflops,
+                      "source": "torch.matmul 4096^3 FP64 and 8192^3 FP32 with TF32 allowed, best of 10, "
+                                "this run"},
             "mixed_over_fp64": value / fp64_value,
             "accuracy": {"rel_err_mixed_max": err_mixed, "rel_err_fp64_max": err_fp64,
                          "rel_diff_mixed_vs_fp64": err_mf, "ranks_identical": ranks_equal,
@@ -391,7 +417,8 @@ def main():
                          "traffic_note": "mean dram read+write per QR-family launch of one 64-TT mixed step (ncu "
                                          "capture of that step); the 768-row randomized-sweep QRs carry it: "
                                          "input and Q exceed L2",
-                         "peak_source": "FP64 cuBLAS DGEMM 4096^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+                         "peak_source": "FP64 torch.matmul (cuBLAS DGEMM) 4096^3, best of 10, measured in this run "
+                                        "(MEASURED_PEAKS.json has no FP64 entry)",
                          "avg_launch_ms": dom_avg_ms, "launches_per_step": dom_n,
                          "profile_ms_per_step": {k: round(v[0], 3) for k, v in prof_m.items() if v[1]},
                          "profile_gflop_per_step": {k: round(v[2] / 1e9, 3) for k, v in prof_m.items() if v[1]}},
@@ -401,7 +428,7 @@ def main():
                     "d2h_bytes_per_step": int(d2h),
                     "path": "DeviceBatch.upload (cores in page-locked host memory, DMA) -> round_rand -> "
                             "download(reuse=True) into page-locked host buffers"},
-            "gpu_launches": int(launches_m * args.steps + launches_f * args.steps),
+            "gpu_launches": int((launches_m + launches_f + launches_t) * args.steps),
             "clocks": clocks,
         }
         if cpu:
