@@ -79,3 +79,38 @@ def test_sketch_precision_names(built_lib):
     assert [ttcuda._sketch_opts(True, 1, None, p, None, keep).precision for p in ("fp64", "bf16", "tf32")] == [0, 1, 2]
     with pytest.raises(ttcuda.ArgumentError):
         ttcuda._sketch_opts(True, 1, None, "fp16", None, keep)
+
+
+def test_ttvector_marshalling_cache(built_lib):
+    """The ctypes view of a TTvector is cached while its core arrays and dims/ranks/ot are the
+    same (in-place core updates keep the pointers valid); replacing a core or changing the ranks
+    rebuilds it, and copies do not carry it."""
+    import copy
+
+    import numpy as np
+    import ttcuda
+    t = ttcuda.TTvector(3, [np.ones((2, 1, 2), order="F"), np.ones((2, 2, 2), order="F"),
+                            np.ones((2, 2, 1), order="F")], (2, 2, 2), [1, 2, 2, 1])
+    keep = ttcuda._Keep()
+    a = ttcuda._ttv(t, keep)
+    cached = t._marshal
+    t.ttv_vec[1][0, 0, 0] = 5.0                     # in place: same arrays, same view
+    ttcuda._ttv(t, keep)
+    assert t._marshal is cached
+    assert C_addr(a.cores, 1) == t.ttv_vec[1].__array_interface__["data"][0]
+    t.ttv_vec[1] = np.zeros((2, 2, 2), order="F")   # replaced core: rebuilt, new pointer
+    b = ttcuda._ttv(t, keep)
+    assert t._marshal is not cached
+    addr = C_addr(b.cores, 1)
+    assert addr == t.ttv_vec[1].__array_interface__["data"][0]
+    t.ttv_rks[1] = 2                                # same values: still cached
+    ttcuda._ttv(t, keep)
+    assert t._marshal[0][2] == (1, 2, 2, 1)
+    assert not hasattr(copy.copy(t), "_marshal") and not hasattr(copy.deepcopy(t), "_marshal")
+    c_ord = ttcuda.TTvector(1, [np.ones((2, 1, 1))], (2,), [1, 1])   # non-Fortran input is converted
+    assert c_ord.ttv_vec[0].flags.f_contiguous
+
+
+def C_addr(pp, i):
+    import ctypes
+    return ctypes.cast(pp[i], ctypes.c_void_p).value
