@@ -630,3 +630,6 @@ class DeviceBatch:
             self.close()
         except Exception:
             pass
+
+
+from .json_io import json_to_mpo, json_to_mps, load_json, mpo_to_json, mps_to_json, save_json  # noqa: E402,F401
