@@ -264,7 +264,7 @@ int ttc_rayleigh_grad(ttc_context* ctx, const ttc_tto* H, const ttc_ttv* x, int3
  * A (lda >= m), Q (m x min(m,n), ldq >= m, may be NULL) and R (min(m,n) x n upper
  * triangular, ldr >= min(m,n), may be NULL) are device pointers on the current device; A
  * is not modified.  Limits: m <= 1536, m*n <= 524288, min(m,n) <= 512, else TTC_EDIM and
- * nothing runs.  Work is queued on `stream` (NULL = default stream) and the call returns
+ * nothing runs; leading dimensions above 2^31 - 1 are refused with TTC_EARG.  Work is queued on `stream` (NULL = default stream) and the call returns
  * without waiting.  `status` (device int32, may be NULL) is zeroed and then receives the
  * kernel flags (2: non-finite value in A).  All calls on a device share the scratch: calls
  * that overlap on the GPU race and must be serialised by the caller.  The first call on a

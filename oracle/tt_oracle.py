@@ -541,7 +541,7 @@ PHILOX_W0, PHILOX_W1 = 0x9E3779B9, 0xBB67AE85
 
 def philox4x32_10(ctr: np.ndarray, key0: int, key1: int) -> np.ndarray:
     """Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).  ctr: uint64 array (n, 4)
-    holding 32-bit words.  Mirrors the device generator in csrc/sketch_gen.cu."""
+    holding 32-bit words.  Mirrors the device generator in tensor-train-julia_b200/csrc/tt_kernels.cu."""
     c = ctr.astype(np.uint64) & 0xFFFFFFFF
     k0 = np.uint64(key0 & 0xFFFFFFFF)
     k1 = np.uint64(key1 & 0xFFFFFFFF)

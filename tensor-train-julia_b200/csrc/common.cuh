@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <stdexcept>
 
@@ -66,6 +67,26 @@ struct GemmDesc {
 };
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+// One-time set-up per device (kernel attributes such as the dynamic shared-memory limit) for
+// launchers that host threads driving different devices may call at the same time: `fn` runs
+// once for each device, under a mutex, before any launch on that device returns from here.
+constexpr int kMaxDevices = 64;
+struct PerDeviceOnce {
+  std::mutex mu;
+  bool done[kMaxDevices] = {};
+  template <class F>
+  void run(int dev, F&& fn) {
+    if (dev < 0 || dev >= kMaxDevices) throw Error(TTC_EARG, "device index out of range");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done[dev]) {
+      fn();
+      done[dev] = true;
+    }
+  }
+};
+// Streaming multiprocessors of the current device (queried once per device, thread-safe).
+int current_sm_count();
 
 // FP32 value rounded to the nearest TF32 (10-bit mantissa, PTX cvt.rna.tf32.f32).  The tensor
 // cores read a kind::tf32 operand by dropping its low 13 mantissa bits (toward zero); operands

@@ -258,13 +258,12 @@ namespace {
 template <bool TF32>
 void launch_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags) {
   const int smem = STAGES * 2 * TILE_BYTES + 1024;
-  static int attr_dev = -1;
+  static PerDeviceOnce attr_once;
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev != dev) {
+  TTC_CUDA(cudaGetDevice(&dev));
+  attr_once.run(dev, [smem] {
     TTC_CUDA(cudaFuncSetAttribute(gemm_bf16_tc_kernel<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr_dev = dev;
-  }
+  });
   gemm_bf16_tc_kernel<TF32><<<(unsigned)total_tiles, NT, smem, s>>>(d, nd, d_flags);
   TTC_CHECK_LAUNCH();
 }

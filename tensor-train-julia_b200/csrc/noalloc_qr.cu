@@ -79,6 +79,9 @@ extern "C" int ttc_qr_noalloc(int32_t m, int32_t n, const double* A, int64_t lda
                                  "min(m,n) <= 512)");
     if (lda < m || (Q && ldq < m) || (R && ldr < K))
       throw ttc::Error(TTC_EARG, "ttc_qr_noalloc: leading dimensions too small");
+    // the kernel descriptor holds 32-bit leading dimensions
+    if (lda > INT32_MAX || (Q && ldq > INT32_MAX) || (R && ldr > INT32_MAX))
+      throw ttc::Error(TTC_EARG, "ttc_qr_noalloc: leading dimensions above 2^31 - 1");
     int dev = 0;
     TTC_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= QRNA_MAX_DEVICES) throw ttc::Error(TTC_EARG, "ttc_qr_noalloc: device index out of range");

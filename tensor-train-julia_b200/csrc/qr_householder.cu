@@ -496,16 +496,14 @@ void launch_qr_apply(const QApplyDesc* d_descs, int count, int max_m, cudaStream
   if (count <= 0) return;
   TTC_REQUIRE(max_m <= QR_MAX_M, TTC_EDIM, "qr apply: row count exceeds the supported maximum (1536)");
   const size_t smem = sizeof(double) * (NB * NB + NW * 128 + (size_t)(max_m + 15) * NB);
-  static int attr_dev = -1;
-  static int nsm = 0;
+  static PerDeviceOnce attr_once;
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev != dev) {
+  TTC_CUDA(cudaGetDevice(&dev));
+  attr_once.run(dev, [] {
     TTC_CUDA(cudaFuncSetAttribute(householder_apply_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(double) * (NB * NB + NW * 128 + (size_t)(QR_MAX_M + 15) * NB))));
-    TTC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    attr_dev = dev;
-  }
+  });
+  const int nsm = current_sm_count();
   int per_sm = 1;
   TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, householder_apply_q_kernel, NT, smem));
   const int csize = std::min(8, std::max(1, nsm * std::max(1, per_sm) / count));
@@ -520,16 +518,14 @@ size_t qr_smem(int max_m) {
 
 void launch_qr_cfg(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags) {
   const size_t smem = qr_smem(max_m);
-  static int attr_dev = -1;
-  static int nsm = 0;
+  static PerDeviceOnce attr_once;
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev != dev) {
+  TTC_CUDA(cudaGetDevice(&dev));
+  attr_once.run(dev, [] {
     TTC_CUDA(cudaFuncSetAttribute(householder_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)qr_smem(QR_MAX_M)));
-    TTC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    attr_dev = dev;
-  }
+  });
+  const int nsm = current_sm_count();
   // CTAs per problem: fill the resident-CTA slots of the GPU, at most 8 (portable cluster)
   int per_sm = 1;
   TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, householder_qr_kernel, NT, smem));

@@ -650,6 +650,17 @@ void ensure_workspace(ttc_context* c, size_t bytes) {
   c->plans.clear();   // descriptors point into the old workspace
 }
 
+int current_sm_count() {
+  static std::mutex mu;
+  static int count[kMaxDevices] = {};
+  int dev = 0;
+  TTC_CUDA(cudaGetDevice(&dev));
+  TTC_REQUIRE(dev >= 0 && dev < kMaxDevices, TTC_EARG, "device index out of range");
+  std::lock_guard<std::mutex> lk(mu);
+  if (count[dev] == 0) TTC_CUDA(cudaDeviceGetAttribute(&count[dev], cudaDevAttrMultiProcessorCount, dev));
+  return count[dev];
+}
+
 void check_device_flags(ttc_context* c) {
   int f = 0;
   TTC_CUDA(cudaMemcpyAsync(&f, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -659,6 +670,7 @@ void check_device_flags(ttc_context* c) {
     if (f & DFLAG_NONFINITE) throw Error(TTC_ENONFINITE, "NaN or Inf met in a factorisation input");
     if (f & DFLAG_JACOBI_NOCONV) throw Error(TTC_ENOCONV, "one-sided Jacobi SVD did not converge within the sweep cap");
     if (f & DFLAG_BAD_DESC) throw Error(TTC_EINTERNAL, "a kernel skipped an inconsistent descriptor");
+    if (f & DFLAG_TIMEOUT) throw Error(TTC_EINTERNAL, "a bounded device wait gave up (tensor-core pipeline stalled)");
   }
 }
 

@@ -528,18 +528,6 @@ __global__ void jacobi_order_kernel(const JacobiDesc* __restrict__ descs, int co
   }
 }
 
-namespace {
-int sm_count() {
-  static int dev_cached = -1, count = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev != dev_cached) {
-    TTC_CUDA(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev));
-    dev_cached = dev;
-  }
-  return count;
-}
-}  // namespace
 
 // Block width and dynamic shared memory of a launch: dyn_doubles(bw, ...) doubles and the
 // active-column list (max_n ints).
@@ -566,7 +554,7 @@ static int jacobi_cluster_size(int count, int max_n, int bw, size_t smem, bool o
   int per_sm = 1;
   TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_svd_kernel<RMAX>, NT, smem));
   per_sm = std::max(1, per_sm);
-  const int slots = sm_count() * per_sm;
+  const int slots = current_sm_count() * per_sm;
   const int pairs = std::max(1, ((max_n + bw - 1) / bw + 1) / 2);
   int c = std::max(1, slots / std::max(1, count));
   if (ordered) c = std::max(c, kOrderedCsize<RMAX>);
@@ -579,13 +567,12 @@ static int jacobi_cluster_size(int count, int max_n, int bw, size_t smem, bool o
 template <int RMAX>
 static void launch_jacobi_t(const JacobiDesc* d_descs, int count, int max_n, int bw, size_t smem, cudaStream_t s,
                             int* d_flags, int* order) {
-  static int attr_dev = -1;
+  static PerDeviceOnce attr_once;
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev != dev) {
+  TTC_CUDA(cudaGetDevice(&dev));
+  attr_once.run(dev, [] {
     TTC_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel<RMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr_dev = dev;
-  }
+  });
   if (order) {
     jacobi_order_kernel<<<1, 512, 0, s>>>(d_descs, count, order);
     TTC_CHECK_LAUNCH();

@@ -217,7 +217,11 @@ def _f64_fortran(c):
 
 def _ttv(x: TTvector, keep: _Keep) -> L.TTV:
     # the marshalled arrays are cached on x while its core arrays (held by the cache, so their
-    # ids stay unique) and its dims/ranks/ot are the same; in-place core updates keep them valid
+    # ids stay unique) and its dims/ranks/ot are the same; in-place core updates keep them valid.
+    # Only views of the user's own arrays are cached: a core that has to be converted (not a
+    # Fortran-ordered float64 array, e.g. one assigned to ttv_vec[k] after construction) is a
+    # private copy that an in-place edit of the user's array would leave stale, so such a TT is
+    # converted afresh on every call.
     key = (tuple(map(id, x.ttv_vec)), tuple(x.ttv_dims), tuple(x.ttv_rks), tuple(x.ttv_ot))
     cached = getattr(x, "_marshal", None)
     if cached is None or cached[0] != key:
@@ -225,7 +229,10 @@ def _ttv(x: TTvector, keep: _Keep) -> L.TTV:
         cores = [_f64_fortran(c) for c in x.ttv_vec]
         args = (_i64(x.ttv_dims, ck), _i64(x.ttv_rks, ck), _i64(x.ttv_ot, ck), _ptrs(cores, ck))
         cached = (key, args, ck, list(x.ttv_vec))
-        x._marshal = cached
+        if all(a is c for a, c in zip(cores, x.ttv_vec)):
+            x._marshal = cached
+        elif hasattr(x, "_marshal"):
+            del x._marshal
     keep.append(cached)
     return L.TTV(x.N, *cached[1])
 

@@ -111,6 +111,28 @@ def test_ttvector_marshalling_cache(built_lib):
     assert c_ord.ttv_vec[0].flags.f_contiguous
 
 
+def test_marshalling_of_converted_core_sees_in_place_edits(built_lib):
+    """A core that is not a Fortran-ordered float64 array (here a C-ordered one assigned after
+    construction) is marshalled as a converted copy: that copy is not cached, so an in-place
+    edit of the user's array reaches the next call instead of a stale copy."""
+    import numpy as np
+    import ttcuda
+    t = ttcuda.TTvector(2, [np.ones((2, 1, 2), order="F"), np.ones((2, 2, 1), order="F")], (2, 2), [1, 2, 1])
+    keep = ttcuda._Keep()
+    ttcuda._ttv(t, keep)
+    assert hasattr(t, "_marshal")
+    core = np.ascontiguousarray(np.arange(4.0).reshape(2, 2, 1))       # C-ordered
+    t.ttv_vec[1] = core
+    a = ttcuda._ttv(t, keep)
+    assert not hasattr(t, "_marshal")
+    first = np.ctypeslib.as_array(ctypes.cast(a.cores[1], ctypes.POINTER(ctypes.c_double)), shape=(4,)).copy()
+    core[1, 0, 0] = 42.0                                                # in-place edit of the user's array
+    b = ttcuda._ttv(t, keep)
+    second = np.ctypeslib.as_array(ctypes.cast(b.cores[1], ctypes.POINTER(ctypes.c_double)), shape=(4,)).copy()
+    assert first[1] == 2.0 and second[1] == 42.0         # column-major (2,2,1): element (1,0,0) is second
+    assert not hasattr(t, "_marshal")
+
+
 def C_addr(pp, i):
     import ctypes
     return ctypes.cast(pp[i], ctypes.c_void_p).value

@@ -40,21 +40,29 @@ def _reference_qr(A):
     return Q, R
 
 
-def _noalloc_qr(A):
+def _noalloc_qr(A, lda=None, want_q=True, want_r=True, want_status=True):
+    """Calls the entry point on device copies of A (leading dimension lda >= m, padding rows
+    filled with NaN so that a read beyond row m would show) and returns Q, R (None when not
+    requested), the status word (None without one) and A's device copy after the call."""
     m, n = A.shape
     K = min(m, n)
+    lda = lda or m
     dev = torch.device("cuda:0")
-    Ad = torch.from_numpy(np.asfortranarray(A).ravel(order="F")).to(dev)
-    Qd = torch.full((m * K,), np.nan, dtype=torch.float64, device=dev)
-    Rd = torch.full((K * n,), np.nan, dtype=torch.float64, device=dev)
-    st = torch.full((1,), -1, dtype=torch.int32, device=dev)
+    Ap = np.full((lda, n), np.nan)
+    Ap[:m] = A
+    Ad = torch.from_numpy(Ap.ravel(order="F").copy()).to(dev)
+    Qd = torch.full((m * K,), np.nan, dtype=torch.float64, device=dev) if want_q else None
+    Rd = torch.full((K * n,), np.nan, dtype=torch.float64, device=dev) if want_r else None
+    st = torch.full((1,), -1, dtype=torch.int32, device=dev) if want_status else None
     torch.cuda.synchronize()
-    rc = lib.ttc_qr_noalloc(m, n, Ad.data_ptr(), m, Qd.data_ptr(), m, Rd.data_ptr(), K, st.data_ptr(), None)
+    rc = lib.ttc_qr_noalloc(m, n, Ad.data_ptr(), lda, Qd.data_ptr() if want_q else None, m,
+                            Rd.data_ptr() if want_r else None, K, st.data_ptr() if want_status else None, None)
     assert rc == 0, lib.ttc_last_error(None).decode()
     torch.cuda.synchronize()
-    Q = Qd.cpu().numpy().reshape((m, K), order="F")
-    R = Rd.cpu().numpy().reshape((K, n), order="F")
-    return Q, R, int(st.cpu().item()), Ad.cpu().numpy()
+    Q = Qd.cpu().numpy().reshape((m, K), order="F") if want_q else None
+    R = Rd.cpu().numpy().reshape((K, n), order="F") if want_r else None
+    status = int(st.cpu().item()) if want_status else None
+    return Q, R, status, Ad.cpu().numpy().reshape((lda, n), order="F")[:m]
 
 
 def test_qr_noalloc_matches_existing_qr_two_calls():
@@ -65,7 +73,7 @@ def test_qr_noalloc_matches_existing_qr_two_calls():
         Q, R, status, A_after = _noalloc_qr(A)
         Qr, Rr = _reference_qr(A)
         assert status == 0
-        assert np.array_equal(A_after.reshape((m, n), order="F"), A)      # input untouched
+        assert np.array_equal(A_after, A)                                 # input untouched
         assert np.allclose(np.tril(R, -1), 0.0)
         # same Householder kernel and sign convention as the existing path: FP64 agreement
         assert np.abs(Q - Qr).max() <= 1e-12
@@ -79,3 +87,61 @@ def test_qr_noalloc_rejects_matrix_beyond_scratch():
     rc = lib.ttc_qr_noalloc(m, n, C.c_void_p(8), m, None, m, None, n, None, None)
     assert rc == 2                                    # TTC_EDIM, nothing launched
     assert b"exceeds the fixed scratch" in lib.ttc_last_error(None)
+
+
+def _check_against_reference(A, Q, R):
+    Qr, Rr = _reference_qr(A)
+    if Q is not None:
+        assert np.abs(Q - Qr).max() <= 1e-12
+    if R is not None:
+        assert np.allclose(np.tril(R, -1), 0.0)
+        assert np.abs(R - Rr).max() <= 1e-12 * np.abs(Rr).max()
+
+
+def test_qr_noalloc_optional_outputs_padded_lda_and_wide_matrix():
+    """Q = NULL, R = NULL, status = NULL (the flags then go to the scratch's own slot), a leading
+    dimension larger than m, and a wide matrix (m < n), each against the existing QR path."""
+    ttcuda.get_context()
+    g = np.random.default_rng(7)
+    A = g.standard_normal((200, 90))
+    _, R, status, _ = _noalloc_qr(A, want_q=False)
+    assert status == 0
+    _check_against_reference(A, None, R)
+    Q, _, status, _ = _noalloc_qr(A, want_r=False)
+    assert status == 0
+    _check_against_reference(A, Q, None)
+    Q, R, status, _ = _noalloc_qr(A, want_status=False)
+    assert status is None
+    _check_against_reference(A, Q, R)
+    Q, R, status, A_after = _noalloc_qr(A, lda=256)
+    assert status == 0 and np.array_equal(A_after, A)
+    _check_against_reference(A, Q, R)
+    W = g.standard_normal((64, 300))                  # wide: K = m, R is 64 x 300
+    Q, R, status, _ = _noalloc_qr(W)
+    assert status == 0
+    _check_against_reference(W, Q, R)
+    assert np.linalg.norm(Q @ R - W) <= 1e-13 * np.linalg.norm(W)
+
+
+def test_qr_noalloc_flags_non_finite_input():
+    """A NaN in A sets flag 2 in the caller's status word; the next call starts from zero."""
+    ttcuda.get_context()
+    A = np.random.default_rng(8).standard_normal((128, 32))
+    A[5, 3] = np.nan
+    _, _, status, _ = _noalloc_qr(A)
+    assert status & 2
+    _, _, status, _ = _noalloc_qr(np.random.default_rng(9).standard_normal((128, 32)))
+    assert status == 0
+
+
+def test_qr_noalloc_rejects_leading_dimension_beyond_int32():
+    """Leading dimensions are stored as 32-bit integers in the kernel descriptor: larger ones are
+    refused before anything runs (no pointer is dereferenced on that path)."""
+    big = 2 ** 31
+    rc = lib.ttc_qr_noalloc(64, 32, C.c_void_p(8), 64, C.c_void_p(8), big, None, 32, None, None)
+    assert rc == 1                                    # TTC_EARG
+    assert b"2^31" in lib.ttc_last_error(None)
+    rc = lib.ttc_qr_noalloc(64, 32, C.c_void_p(8), 64, None, 64, C.c_void_p(8), big, None, None)
+    assert rc == 1
+    rc = lib.ttc_qr_noalloc(64, 32, C.c_void_p(8), big, None, 64, None, 32, None, None)
+    assert rc == 1
