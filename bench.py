@@ -74,15 +74,23 @@ def make_tt(dims, ranks, seed, decay_per=32.0):
     return vec
 
 
-def workload(seed, batch=BATCH):
+def batch_ranks(seed, batch=BATCH):
+    """Rank lists of the batch's TTs: interior ranks i.i.d. U[RMIN, RMAX] per TT and bond, clamped."""
     g = np.random.default_rng(seed)
     dims = (NPHYS,) * D
-    tts = []
-    for i in range(batch):
+    out = []
+    for _ in range(batch):
         r = [1] + [int(v) for v in g.integers(RMIN, RMAX + 1, size=D - 1)] + [1]
-        r = r_and_d(r, dims, max(r))
-        tts.append((dims, r, make_tt(dims, r, seed * 100003 + i)))
-    return dims, tts
+        out.append(r_and_d(r, dims, max(r)))
+    return dims, out
+
+
+def workload(seed, batch=BATCH, indices=None):
+    """The batch's TTs (all, or those at `indices`): TT i has its own generator seed, so any subset
+    is generated without the others."""
+    dims, ranks = batch_ranks(seed, batch)
+    idx = range(batch) if indices is None else indices
+    return dims, [(dims, ranks[i], make_tt(dims, ranks[i], seed * 100003 + i)) for i in idx]
 
 
 def heuristic(rank_lists):
@@ -145,18 +153,33 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU baselines
-def cpu_reference_rate(dims, tts, rks, sample):
+def cpu_reference_rate(dims, tts, rks, sample, start=0):
     """The FP64 CPU restatement of the reference path (ttrand_rounding + tt_rounding, LAPACK via
-    numpy/scipy on all host cores) on `sample` TTs of the batch; returns (roundings/s, seconds)."""
+    numpy/scipy on all host cores) on `sample` TTs of the batch from index `start` (cyclically);
+    returns (roundings/s, seconds, rounded TTs)."""
     sys.path.insert(0, ROOT)
     from oracle import tt_oracle as o
+    outs = []
     t0 = time.perf_counter()
-    for dims_i, r, vec in tts[:sample]:
+    for i in range(sample):
+        dims_i, r, vec = tts[(start + i) % len(tts)]
         x = o.TTvector(len(dims_i), [c.copy() for c in vec], tuple(dims_i), list(r), [0] * len(dims_i))
         y = o.ttrand_rounding(x, rks, orthogonal=True, seed=1234, block_rks=len(dims_i))
-        o.tt_rounding(y, tol=TOL)
+        outs.append(o.tt_rounding(y, tol=TOL))
     dt = time.perf_counter() - t0
-    return sample / dt, dt
+    return sample / dt, dt, outs
+
+
+def oracle_comparison(oracle_outs, gpu_outs):
+    """Largest ||y_gpu - y_oracle|| / ||y_oracle|| over the TTs both sides rounded (FP64 norm of the
+    difference TT, computed by the oracle) and whether all truncation ranks are identical."""
+    from oracle import tt_oracle as o
+    diffs, same = [], True
+    for yo, yg in zip(oracle_outs, gpu_outs):
+        g = o.TTvector(yg.N, [np.asarray(c) for c in yg.ttv_vec], tuple(yg.ttv_dims), list(yg.ttv_rks), [0] * yg.N)
+        same = same and list(yo.ttv_rks) == list(g.ttv_rks)
+        diffs.append(o.rel_error(yo, g))
+    return max(diffs), same
 
 
 # ---------------------------------------------------------------------- reference arm
@@ -168,13 +191,13 @@ def run_reference(args, rank):
     sample = max(1, int(os.environ.get("TTC_REF_SAMPLE", "3")))
     for _ in range(max(0, min(args.warmup, 1))):
         cpu_reference_rate(dims, tts, rks, 1)
-    rates = []
     t_all = time.perf_counter()
-    for _ in range(args.steps):
-        r, _ = cpu_reference_rate(dims, tts, rks, sample)
-        rates.append(r)
+    for step in range(args.steps):
+        # the sample moves through the batch (step i rounds TTs sample*i ...), so that the rate is
+        # not that of the same few rank draws every step
+        cpu_reference_rate(dims, tts, rks, sample, start=step * sample)
     total = time.perf_counter() - t_all
-    v = float(np.mean(rates))
+    v = float(sample * args.steps / total)
     cores = os.cpu_count() or 1
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "roundings/s", "n_gpus": args.gpus,
@@ -182,9 +205,10 @@ def run_reference(args, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "batched rounding: 64 TTs, d=32, n=2, ranks U[16,256], sigma 10^(-i/32), tol 1e-8",
                    "variant": "FP64 ttrand_rounding + tt_rounding (reference algorithm, CPU restatement)",
-                   "sample": f"{sample} TT(s) of the batch per step"},
+                   "sample": f"{sample} TT(s) of the batch per step, the next {sample} each step (cyclic)"},
         "cpu_baseline": {"value": v, "unit": "roundings/s", "cores": cores, "kind": "port",
-                         "sample": f"{sample} TT(s) per step (CPU restatement of the Julia path; Julia is absent)"},
+                         "sample": f"{sample} TT(s) per step, moving through the 64-TT batch "
+                                   "(CPU restatement of the Julia path; Julia is absent)"},
         "e2e": {"value": v, "unit": "roundings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -224,10 +248,14 @@ def main():
     ctx.set_stream(stream.cuda_stream)
     ttcuda._CTX = ctx
 
-    dims, tts = workload(seed=shard.rank_seed(7, rank), batch=args.batch)
+    # one job of batch x world TTs, partitioned over the ranks by estimated work (sum of r_k^3)
+    job = args.batch * world
+    _, job_ranks = batch_ranks(7, job)
+    mine = shard.shard_by_work([shard.tt_work(r) for r in job_ranks], world)[rank]
+    dims, tts = workload(seed=7, batch=job, indices=mine)
     ranks = [r for _, r, _ in tts]
     tt_objs = [ttcuda.TTvector(len(d_), v, d_, r, [0] * len(d_)) for d_, r, v in tts]
-    rks = heuristic(ranks)
+    rks = heuristic(job_ranks)              # the whole job's default_rank_heuristic
     block = D                        # ttrand_rounding's default block_rks = N
     s = ttcuda._sketch_ranks(dims, rks, block)
     rho = ttcuda._rand_out_caps(dims, s)
@@ -282,10 +310,9 @@ def main():
     ctx.synchronize()
     clocks = cs.summary(local)
 
-    nb = len(tts) * world
-    value = shard.whole_job_rate(len(tts), world, args.steps, ms_mixed)
-    fp64_value = shard.whole_job_rate(len(tts), world, args.steps, ms_fp64)
-    tf32_value = shard.whole_job_rate(len(tts), world, args.steps, ms_tf32)
+    value = shard.job_rate(job, args.steps, ms_mixed)
+    fp64_value = shard.job_rate(job, args.steps, ms_fp64)
+    tf32_value = shard.job_rate(job, args.steps, ms_tf32)
 
     # accuracy on the GPU: ||x - round(x)|| / ||x|| through the library (difference TT, norm)
     def rel_err(x, y):
@@ -375,22 +402,29 @@ def main():
     e1.record(stream)
     barrier()
     e2e_ms = shard.max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
-    e2e_value = shard.whole_job_rate(len(tts), world, args.steps, e2e_ms)
+    e2e_value = shard.job_rate(job, args.steps, e2e_ms)
 
     cpu = None
+    oracle_cmp = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, secs = cpu_reference_rate(dims, tts, rks, 3)
+        rate, secs, ref_outs = cpu_reference_rate(dims, tts, rks, 3)
         cpu = {"value": rate, "unit": "roundings/s", "cores": os.cpu_count() or 1, "kind": "port",
                "sample": f"first 3 TTs of the batch ({secs:.1f} s): FP64 ttrand_rounding + tt_rounding, "
                          "numpy/LAPACK on all host threads"}
+        # the same 3 TTs rounded by the GPU (mixed and FP64 variants) against the oracle's results
+        d_m, same_m = oracle_comparison(ref_outs, out_m[:3])
+        d_f, same_f = oracle_comparison(ref_outs, out_f[:3])
+        oracle_cmp = {"rel_diff_vs_oracle": d_m, "ranks_identical_oracle": same_m,
+                      "fp64_rel_diff_vs_oracle": d_f, "fp64_ranks_identical_oracle": same_f, "checked_tts": 3,
+                      "oracle": "FP64 restatement, same Philox sketch blocks (seed 1234)"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "roundings/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16 sketch + f64", "data": "synthetic",
-            "config": {"workload": f"batched rounding: {len(tts)} TTs per GPU, d=32, n=2, ranks U[16,256] (seeded), "
-                                   "sigma 10^(-i/32), tol 1e-8",
+            "config": {"workload": f"batched rounding: {job} TTs ({args.batch} per GPU, partitioned by sum of r^3), "
+                                   "d=32, n=2, ranks U[16,256] (seeded), sigma 10^(-i/32), tol 1e-8",
                        "variant": "mixed: BF16-sketch (tcgen05) ttrand_rounding + FP64 SVD sweep",
                        "sketch_ranks": "default_rank_heuristic of the batch (r + ceil(max r/2)); block_rks = N, "
                                        "orthogonal blocks, seed 1234 (ttrand_rounding defaults)",
@@ -433,6 +467,8 @@ def main():
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if oracle_cmp:
+            line["accuracy"].update(oracle_cmp)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -22,6 +22,45 @@ import scipy.linalg as sla
 F = "F"
 
 
+def ein(expr: str, *ops: np.ndarray) -> np.ndarray:
+    """Contraction of `ops` by the index expression `expr` (einsum notation), performed pairwise
+    from left to right -- the operands' order is the contraction order, as in the reference's
+    hand-ordered `mul!` chains -- each step a BLAS tensordot over the indices no later operand
+    or the output needs (an index shared by both sides and still needed later falls back to a
+    two-operand einsum)."""
+    ins, out = expr.split("->")
+    subs = ins.split(",")
+    assert len(subs) == len(ops)
+
+    def needed(k):
+        return set(out) | set("".join(subs[k + 1:]))
+
+    def reduce_alone(s, A, keep):
+        drop = [c for c in s if c not in keep and s.count(c) == 1]
+        if drop:
+            A = A.sum(axis=tuple(s.index(c) for c in drop))
+            s = "".join(c for c in s if c not in drop)
+        return s, A
+
+    cur_s, cur = reduce_alone(subs[0], ops[0], needed(0) | set(subs[1]) if len(subs) > 1 else set(out))
+    for k in range(1, len(ops)):
+        s, B = subs[k], ops[k]
+        later = needed(k)
+        s, B = reduce_alone(s, B, later | set(cur_s))
+        shared = [c for c in cur_s if c in s]
+        summed = [c for c in shared if c not in later]
+        batch = [c for c in shared if c in later]
+        if batch:
+            res = "".join(dict.fromkeys(c for c in cur_s + s if c in later))
+            cur = np.einsum(f"{cur_s},{s}->{res}", cur, B)
+            cur_s = res
+        else:
+            cur = np.tensordot(cur, B, axes=([cur_s.index(c) for c in summed], [s.index(c) for c in summed]))
+            cur_s = "".join(c for c in cur_s if c not in summed) + "".join(c for c in s if c not in summed)
+    cur_s, cur = reduce_alone(cur_s, cur, set(out))
+    return np.ascontiguousarray(np.transpose(cur, [cur_s.index(c) for c in out]))
+
+
 # --------------------------------------------------------------------------- types
 @dataclass
 class TTvector:
@@ -371,7 +410,7 @@ def dot(A: TTvector, B: TTvector) -> float:
     assert tuple(A.ttv_dims) == tuple(B.ttv_dims)
     out = np.ones((1, 1))
     for k in range(A.N):
-        out = np.einsum("zab,zcd,ac->bd", A.ttv_vec[k], np.conj(B.ttv_vec[k]), out)
+        out = ein("ac,zab,zcd->bd", out, A.ttv_vec[k], np.conj(B.ttv_vec[k]))
     return float(out[0, 0])
 
 
@@ -382,11 +421,11 @@ def partial_contraction(A: TTvector, B: TTvector, reverse=True) -> List[np.ndarr
     if reverse:
         W[L] = np.ones((1, 1))
         for k in range(L - 1, -1, -1):
-            W[k] = np.einsum("zab,zcd,bd->ac", A.ttv_vec[k], B.ttv_vec[k], W[k + 1])
+            W[k] = ein("bd,zab,zcd->ac", W[k + 1], A.ttv_vec[k], B.ttv_vec[k])
     else:
         W[0] = np.ones((1, 1))
         for k in range(L):
-            W[k + 1] = np.einsum("zab,zcd,ac->bd", A.ttv_vec[k], B.ttv_vec[k], W[k])
+            W[k + 1] = ein("ac,zab,zcd->bd", W[k], A.ttv_vec[k], B.ttv_vec[k])
     return W
 
 
@@ -399,12 +438,12 @@ def dot_operator(psi: TTvector, H: TToperator, phi: TTvector) -> float:
     c = max(center(psi), center(phi))
     L = np.ones((1, 1, 1))
     for k in range(c if c > 1 else 0):
-        L = np.einsum("abc,iad,ijbe,jcf->def", L, np.conj(psi.ttv_vec[k]), H.tto_vec[k], phi.ttv_vec[k])
+        L = ein("abc,iad,ijbe,jcf->def", L, np.conj(psi.ttv_vec[k]), H.tto_vec[k], phi.ttv_vec[k])
     R = np.ones((1, 1, 1))
     r = c + 1 if c > 1 else 1
     for k in range(N, r - 1, -1):
         kk = k - 1
-        R = np.einsum("iad,ijbe,jcf,def->abc", np.conj(psi.ttv_vec[kk]), H.tto_vec[kk], phi.ttv_vec[kk], R)
+        R = ein("def,jcf,ijbe,iad->abc", R, phi.ttv_vec[kk], H.tto_vec[kk], np.conj(psi.ttv_vec[kk]))
     if c == 1:
         res = R
     elif c == N:
@@ -532,6 +571,25 @@ def tt_rounding(x: TTvector, tol=1e-12, rmax=2 ** 14, direction="left") -> TTvec
 def tt_rounding_tto(A: TToperator, tol=1e-12, rmax=2 ** 14) -> TToperator:
     """src/tt_rounding.jl:275-277"""
     return ttv_to_tto(tt_rounding(tto_to_ttv(A), tol=tol, rmax=rmax))
+
+
+def tt_svdvals(x: TTvector, tol: float = 0.0) -> List[np.ndarray]:
+    """src/tt_rounding.jl:282-295: singular values of the unfolding x[mu_1..mu_k; mu_{k+1}..mu_d]
+    for k = 1..N-1 (orthogonalize onto site 1, then an L->R SVD sweep).  tol = 0 keeps every
+    singular value (floor(s, 0) returns s); the reference's default 1e-14 applies the floor rule."""
+    N = x.N
+    y = orthogonalize(x, i=1)
+    out = []
+    cur = y.ttv_vec[0].reshape(y.ttv_dims[0] * y.ttv_rks[0], y.ttv_rks[1], order=F)
+    for j in range(N - 1):
+        u, s, vh = svd_julia(cur)
+        k = floor_rank(s, tol) if tol > 0 else len(s)
+        out.append(np.array(s[:k]))
+        nxt = y.ttv_vec[j + 1]                               # (n, r_j, r_{j+1})
+        SV = s[:, None] * vh                                 # (len(s), r_j)
+        core = np.einsum("az,izb->iab", SV, nxt)
+        cur = core.reshape(core.shape[0] * core.shape[1], core.shape[2], order=F)
+    return out
 
 
 # ------------------------------------------------------------- sketch generation
@@ -681,13 +739,24 @@ def make_reverse_sketch(dims, rks, seed=1234, orthogonal=True, block_rks=None, p
 
 
 def contract_sketch_core_backwards(A: np.ndarray, S: np.ndarray, V: np.ndarray) -> np.ndarray:
-    """src/sketches.jl:1602-1638: W[a,b] = sum A[z,a,al] S[be,z,b] V[al,be]."""
-    return np.einsum("zaA,Bzb,AB->ab", A, S, V, optimize=True)
+    """src/sketches.jl:1602-1638: W[a,b] = sum A[z,a,al] S[be,z,b] V[al,be], in the order the
+    reference's cost test picks: (A V) S or A (V S)."""
+    z, a, al = A.shape
+    be, _, b = S.shape
+    if a * be * (al + b + 1) < al * (b + 1) * (a + be):
+        return ein("zaA,AB,Bzb->ab", A, V, S)
+    return ein("AB,Bzb,zaA->ab", V, S, A)
 
 
 def contract_sketch_core_backwards_op(A, B, S, V):
-    """src/sketches.jl:1648-1713: W[a,b,c] = sum A[z,a,al] B[ze,z,b,be] S[ga,ze,c] V[al,be,ga]."""
-    return np.einsum("zaA,Zzbe,gZc,Aeg->abc", A, B, S, V, optimize=True)
+    """src/sketches.jl:1648-1713: W[a,b,c] = sum A[z,a,al] B[ze,z,b,be] S[ga,ze,c] V[al,be,ga], in
+    the order the reference's cost test picks: ((V A) B) S or ((V S) B) A."""
+    z, a, al = A.shape
+    ze, _, b, be = B.shape
+    ga, _, c = S.shape
+    if a * ga * (z * be * (al + ze * b) + ze * b * c) < al * c * (ze * be * (ga + z * b) + z * a * b):
+        return ein("Aeg,zaA,Zzbe,gZc->abc", V, A, B, S)
+    return ein("Aeg,gZc,Zzbe,zaA->abc", V, S, B, A)
 
 
 def tt_recursive_sketch(A: TTvector, rks, orthogonal=True, seed=1234, block_rks=None, p=None,
@@ -770,7 +839,7 @@ def ttrand_rounding(y: TTvector, rks=None, orthogonal=True, seed=1234, block_rks
         out_rks[k + 1] = Q.shape[1]
         vec[k] = Q.reshape(dims[k], out_rks[k], out_rks[k + 1], order=F)
         ot[k] = 1
-        yk = np.einsum("iab,iac,jbd->jcd", yk, vec[k], y.ttv_vec[k + 1], optimize=True)
+        yk = ein("iab,iac,jbd->jcd", yk, vec[k], y.ttv_vec[k + 1])
     vec[N - 1] = yk.reshape(dims[N - 1], out_rks[N - 1], out_rks[N], order=F)
     return TTvector(N, vec, tuple(dims), out_rks, ot)
 
@@ -806,7 +875,7 @@ def ttrand_rounding_lincomb(alpha: Sequence[float], ys: Sequence[TTvector], rks=
         out_rks[k + 1] = Q.shape[1]
         vec[k] = Q.reshape(dims[k], out_rks[k], out_rks[k + 1], order=F)
         ot[k] = 1
-        Yk = [np.einsum("iab,iac,jbd->jcd", Yk[j], vec[k], ys[j].ttv_vec[k + 1], optimize=True) for j in range(m)]
+        Yk = [ein("iab,iac,jbd->jcd", Yk[j], vec[k], ys[j].ttv_vec[k + 1]) for j in range(m)]
     out_rks[N] = 1
     vec[N - 1] = sum(Yk)
     return TTvector(N, vec, tuple(dims), out_rks, ot)
@@ -846,10 +915,10 @@ def ttrand_rounding_op(alpha: Sequence[float], H: TToperator, ys: Sequence[TTvec
         vec[k] = Q.reshape(dims[k], out_rks[k], out_rks[k + 1], order=F)
         ot[k] = 1
         y1k = Yk[0].reshape(dims[k], out_rks[k], ys[0].ttv_rks[k + 1], H.tto_rks[k + 1], order=F)
-        Ay = np.einsum("irab,irs,jac,ljbd->lscd", y1k, vec[k], ys[0].ttv_vec[k + 1], H.tto_vec[k + 1], optimize=True)
+        Ay = ein("irab,irs,jac,ljbd->lscd", y1k, vec[k], ys[0].ttv_vec[k + 1], H.tto_vec[k + 1])
         new = [Ay.reshape(dims[k + 1], out_rks[k + 1], ys[0].ttv_rks[k + 2] * H.tto_rks[k + 2], order=F)]
         for j in range(1, m):
-            new.append(np.einsum("iab,iac,jbd->jcd", Yk[j], vec[k], ys[j].ttv_vec[k + 1], optimize=True))
+            new.append(ein("iab,iac,jbd->jcd", Yk[j], vec[k], ys[j].ttv_vec[k + 1]))
         Yk = new
     out_rks[N] = 1
     vec[N - 1] = sum(Yk)
@@ -879,8 +948,8 @@ def ttrand_rounding_residual(Atto: TToperator, y: TTvector, b: TTvector, rks=Non
         out_rks[k + 1] = Q.shape[1]
         vec[k] = Q.reshape(dims[k], out_rks[k], out_rks[k + 1], order=F)
         ot[k] = 1
-        Ayk = np.einsum("irab,irs,jac,ljbd->lscd", Ayk, vec[k], y.ttv_vec[k + 1], Atto.tto_vec[k + 1], optimize=True)
-        bk = np.einsum("ira,irs,jab->jsb", bk, vec[k], b.ttv_vec[k + 1], optimize=True)
+        Ayk = ein("irab,irs,jac,ljbd->lscd", Ayk, vec[k], y.ttv_vec[k + 1], Atto.tto_vec[k + 1])
+        bk = ein("ira,irs,jab->jsb", bk, vec[k], b.ttv_vec[k + 1])
     vec[N - 1] = Ayk.reshape(dims[N - 1], out_rks[N - 1], 1, order=F) - bk.reshape(dims[N - 1], out_rks[N - 1], 1, order=F)
     return TTvector(N, vec, tuple(dims), out_rks, ot)
 
@@ -898,22 +967,22 @@ def rayleigh_value_and_grad(H: TToperator, x: TTvector):
     Lh[0] = np.ones((1, 1, 1))
     Ln[0] = np.ones((1, 1))
     for k in range(N):
-        Lh[k + 1] = np.einsum("abc,iad,ijbe,jcf->def", Lh[k], x.ttv_vec[k], H.tto_vec[k], x.ttv_vec[k], optimize=True)
-        Ln[k + 1] = np.einsum("ac,iad,icf->df", Ln[k], x.ttv_vec[k], x.ttv_vec[k], optimize=True)
+        Lh[k + 1] = ein("abc,iad,ijbe,jcf->def", Lh[k], x.ttv_vec[k], H.tto_vec[k], x.ttv_vec[k])
+        Ln[k + 1] = ein("ac,iad,icf->df", Ln[k], x.ttv_vec[k], x.ttv_vec[k])
     Rh = [None] * (N + 1)
     Rn = [None] * (N + 1)
     Rh[N] = np.ones((1, 1, 1))
     Rn[N] = np.ones((1, 1))
     for k in range(N - 1, -1, -1):
-        Rh[k] = np.einsum("iad,ijbe,jcf,def->abc", x.ttv_vec[k], H.tto_vec[k], x.ttv_vec[k], Rh[k + 1], optimize=True)
-        Rn[k] = np.einsum("iad,icf,df->ac", x.ttv_vec[k], x.ttv_vec[k], Rn[k + 1], optimize=True)
+        Rh[k] = ein("def,jcf,ijbe,iad->abc", Rh[k + 1], x.ttv_vec[k], H.tto_vec[k], x.ttv_vec[k])
+        Rn[k] = ein("df,icf,iad->ac", Rn[k + 1], x.ttv_vec[k], x.ttv_vec[k])
     e = float(Lh[N].reshape(-1)[0])
     nn = float(Ln[N].reshape(-1)[0])
     R = e / nn
     grads = []
     for k in range(N):
-        hx = np.einsum("abc,ijbe,jcf,def->iad", Lh[k], H.tto_vec[k], x.ttv_vec[k], Rh[k + 1], optimize=True)
-        nx = np.einsum("ac,icf,df->iad", Ln[k], x.ttv_vec[k], Rn[k + 1], optimize=True)
+        hx = ein("abc,jcf,ijbe,def->iad", Lh[k], x.ttv_vec[k], H.tto_vec[k], Rh[k + 1])
+        nx = ein("ac,icf,df->iad", Ln[k], x.ttv_vec[k], Rn[k + 1])
         grads.append((2.0 / nn) * (hx - R * nx))
     return R, grads
 
