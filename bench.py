@@ -415,7 +415,7 @@ def main():
         d_m, same_m = oracle_comparison(ref_outs, out_m[:3])
         d_f, same_f = oracle_comparison(ref_outs, out_f[:3])
         oracle_cmp = {"rel_diff_vs_oracle": d_m, "ranks_identical_oracle": same_m,
-                      "fp64_rel_diff_vs_oracle": d_f, "fp64_ranks_identical_oracle": same_f, "checked_tts": 3,
+                      "fp64_rel_diff_vs_oracle": d_f, "fp64_ranks_identical_oracle": same_f, "oracle_checked_tts": 3,
                       "oracle": "FP64 restatement, same Philox sketch blocks (seed 1234)"}
 
     if rank == 0:

@@ -126,6 +126,11 @@ typedef struct {
   /* execution plans built since the context was created (a repeated call with the same
    * shapes reuses its plan and replays it as a CUDA graph) */
   int64_t plans_built;
+  /* roundings run a second time because the Jacobi SVD hit its sweep cap (TTC_ENOCONV): the
+   * synchronous entry points then retry once with four times the cap, as the reference retries a
+   * failed gesdd with QR iteration (src/tt_rounding.jl:191-195); counted since the context was
+   * created.  The asynchronous entry points report TTC_ENOCONV from ttc_synchronize instead. */
+  int64_t svd_retries;
 } ttc_stats;
 
 /* Per-kernel-family timing of subsequent calls (0 = off, the default). */

@@ -19,6 +19,33 @@ std::vector<const double*> upload_host_blocks(ttc_context* c, const std::vector<
                                               const double* const* blocks, std::string& key);
 std::vector<long long> rks_vec(const int64_t* rks, int N);
 
+// Sets the Jacobi SVD sweep cap of later launches; plans hold the cap, so they are rebuilt.
+void set_jacobi_max_sweeps(ttc_context* c, int sweeps);
+
+// Runs a synchronous rounding `run` (which raises the device flags itself); if the Jacobi SVD
+// hit its sweep cap (TTC_ENOCONV), runs it once more with four times the cap, as the reference
+// retries a failed gesdd with QR iteration (src/tt_rounding.jl:191-195).  `run` must start from
+// inputs the first pass did not modify (roundings write a separate output batch).  A second
+// failure is reported as TTC_ENOCONV.
+template <class F>
+void with_svd_retry(ttc_context* c, F&& run) {
+  try {
+    run();
+  } catch (const Error& e) {
+    if (e.status != TTC_ENOCONV) throw;
+    const int cap0 = c->jacobi_max_sweeps;
+    c->stats.svd_retries += 1;
+    set_jacobi_max_sweeps(c, cap0 * 4);
+    try {
+      run();
+    } catch (...) {
+      set_jacobi_max_sweeps(c, cap0);
+      throw;
+    }
+    set_jacobi_max_sweeps(c, cap0);
+  }
+}
+
 struct BatchHolder {
   std::vector<ttc_batch*> v;
   ~BatchHolder() { for (auto* b : v) batch_destroy(b); }

@@ -335,6 +335,14 @@ ttc_batch* batch_empty_like(ttc_context* c, int count, int N, const std::vector<
 
 
 
+void set_jacobi_max_sweeps(ttc_context* c, int sweeps) {
+  TTC_REQUIRE(sweeps >= 1, TTC_EARG, "the Jacobi sweep cap must be at least 1");
+  if (c->jacobi_max_sweeps == sweeps) return;
+  TTC_CUDA(cudaStreamSynchronize(c->stream));     // no plan of the old cap still running
+  c->jacobi_max_sweeps = sweeps;
+  c->plans.clear();
+}
+
 void record_stats(ttc_context* c, int nstages) {
   TTC_CUDA(cudaStreamSynchronize(c->stream));
   // an event pair that cannot be timed reports 0 (its error is consumed here, so that it is
@@ -573,9 +581,11 @@ size_t ttc_batch_bytes(const ttc_batch* b) {
 int ttc_batch_round_det(ttc_context* c, ttc_batch* x, const ttc_round_opts* opts, ttc_batch* y) {
   if (!c || !x || !y || !opts) return TTC_EARG;
   return guard(c, [&] {
-    round_det(c, x, *opts, y);
-    record_stats(c, 3);
-    check_device_flags(c);
+    with_svd_retry(c, [&] {
+      round_det(c, x, *opts, y);
+      record_stats(c, 3);
+      check_device_flags(c);
+    });
   });
 }
 
@@ -591,9 +601,11 @@ int ttc_batch_round_rand(ttc_context* c, ttc_batch* x, const int64_t* rks, const
     std::string key;
     const auto r = rks_vec(rks, x->N);
     const auto raw = upload_host_blocks(c, x->dims, sketch_plan(x->dims, r, sk->block_rks), sk->sketch_blocks, key);
-    round_rand(c, x, r, *sk, after, y, raw, key);
-    record_stats(c, 4);
-    check_device_flags(c);
+    with_svd_retry(c, [&] {
+      round_rand(c, x, r, *sk, after, y, raw, key);
+      record_stats(c, 4);
+      check_device_flags(c);
+    });
   });
 }
 

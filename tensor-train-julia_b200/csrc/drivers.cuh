@@ -38,8 +38,12 @@ inline void check_precision(int p) {
               "sketch precision must be TTC_PREC_FP64, TTC_PREC_BF16 or TTC_PREC_TF32");
 }
 inline bool tensor_core_sketch(int p) { return p == TTC_PREC_BF16 || p == TTC_PREC_TF32; }
+// `complete`: write the completion columns of rank-deficient range finders (false when a truncated-SVD
+// sweep follows in the same plan); `eff` (optional) receives the effective ranks the cores are
+// nonzero within.
 void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<int>& tts, const SketchPlan& sp,
-                     const std::vector<std::vector<double*>>& W, const std::vector<std::vector<int>>& rho);
+                     const std::vector<std::vector<double*>>& W, const std::vector<std::vector<int>>& rho,
+                     bool complete = true, std::vector<std::vector<int>>* eff = nullptr);
 std::vector<int> orth_left_ranks(const ttc_batch* x, int t);
 std::vector<int> rand_out_ranks(const std::vector<long long>& dims, const SketchPlan& sp);
 bool is_left_orth(const ttc_batch* x, int t);

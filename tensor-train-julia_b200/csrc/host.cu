@@ -28,9 +28,11 @@ void tt_rounding_host(ttc_context* c, const ttc_ttv* x, const ttc_round_opts& o,
   ttc_batch* yb = H.add(batch_create(c, 1, N, xb->dims.data(), cap.data()));
   ttc_round_opts lo = o;
   lo.direction = TTC_DIR_LEFT;
-  round_det(c, xb, lo, yb);
-  record_stats(c, 3);
-  check_device_flags(c);
+  with_svd_retry(c, [&] {
+    round_det(c, xb, lo, yb);
+    record_stats(c, 3);
+    check_device_flags(c);
+  });
   batch_download_many(yb, 0, 1, y, rev);
 }
 
@@ -57,9 +59,11 @@ void rand_rounding_host(ttc_context* c, int m, const double* alpha, const ttc_tt
   check_precision(sk.precision);
   std::string key;
   const auto raw = upload_host_blocks(c, xb->dims, sp, sk.sketch_blocks, key);
-  round_rand(c, xb, r, sk, after, yb, raw, key);
-  record_stats(c, 4);
-  check_device_flags(c);
+  with_svd_retry(c, [&] {
+    round_rand(c, xb, r, sk, after, yb, raw, key);
+    record_stats(c, 4);
+    check_device_flags(c);
+  });
   batch_download_many(yb, 0, 1, y, false);
 }
 

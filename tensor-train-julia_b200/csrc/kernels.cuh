@@ -64,8 +64,10 @@ struct JacobiDesc {
 // their size (rows after the device bound x columns^2, largest first) so that the clusters,
 // which the hardware starts in index order, take the longest problems first.
 constexpr int kJacobiOrderMax = 4096;
+// max_sweeps: sweep cap; a problem still rotating after it sets DFLAG_JACOBI_NOCONV.
+constexpr int kJacobiDefaultSweeps = 40;
 void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, bool accw, cudaStream_t s,
-                   int* d_flags, int* order = nullptr);
+                   int* d_flags, int* order = nullptr, int max_sweeps = kJacobiDefaultSweeps);
 
 // ---- truncation rule (tt_kernels.cu): floor(s, tol) then min(k, rmax, #(s>0))
 struct TruncDesc {

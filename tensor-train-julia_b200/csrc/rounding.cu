@@ -405,53 +405,152 @@ void emit_sketch_f64(Builder& B, ttc_batch* x, const std::vector<int>& tts, cons
   }
 }
 
-// Left-to-right orthogonalise-and-project sweep of ttrand_rounding
-// (src/tt_randtools.jl:123-151) for single TTs: Z = y_k W_{k+1}, Q = qr(Z), y_{k+1} = Q^T y_k A_{k+1}.
+// Left-to-right orthogonalise-and-project sweep of ttrand_rounding (src/tt_randtools.jl:123-151):
+// Z = y_k W_{k+1}, Q = qr(Z) (thin Householder Q), core k = Q, y_{k+1} = Q^T y_k A_{k+1}.
+//
+// y_k is kept compact: only its first e_k left indices can be nonzero (e_0 = 1), stored as
+// (e_k, n, r_{k+1}), so its unfolding Y is m x c with m = n e_k and c = r_{k+1}.  Z = Y W has
+// rank q <= min(m, c, s) (s = sketch rank of bond k+1), and the Householder QR of Z is formed
+// three ways, all giving the same first q columns (up to the reflectors' sign convention, which
+// is LAPACK's in each QR):
+//  * F (q = s: Z has full column rank, the randomized compression case): Z is formed and
+//    factored as the reference does.
+//  * T (q = c < m, s: more sketch columns than Y has columns): Z = Y W = Q1 (R1 W).  Householder
+//    QR of Z factors its columns left to right, so its first c columns are the QR of
+//    Z[:, :c] = Q1 M1 with M1 = R1 W[:, :c]: Q1 Q_M, Q_M the Q of the c x c matrix M1.  The
+//    columns beyond c (Z's numerical null space: there LAPACK orthonormalises rounding noise)
+//    are completed deterministically: the reflectors of Y applied to unit vectors, then unit
+//    vectors in y_k's zero rows.
+//  * W (q = m <= c, m < s): Q1 = I, M1 = Y W[:, :m], and core k's first m columns are Q_M.
+// Then Q^T y_k = [Q_M^T R1; 0] (T) or [Q_M^T Y; 0] (W): y_{k+1} has e_{k+1} = q nonzero rows.
+// The represented tensor is the reference's: range(Q) contains range(y_k), and the completion
+// columns meet zero rows of y_{k+1}.  When the truncated-SVD sweep follows in the same plan
+// (`complete` false) the completion columns are not written: the sweep reads cores only up to
+// the effective ranks e, which `eff` returns, and the cores must stay zero beyond their ranks.
 void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<int>& tts, const SketchPlan& sp,
-                     const std::vector<std::vector<double*>>& W, const std::vector<std::vector<int>>& rho) {
+                     const std::vector<std::vector<double*>>& W, const std::vector<std::vector<int>>& rho,
+                     bool complete, std::vector<std::vector<int>>* eff) {
   const int N = x->N;
   const size_t T = tts.size();
   std::vector<double*> Y(T), Yn(T);
-  std::vector<int> yld(T);
+  std::vector<int> e(T, 1);
+  if (eff) eff->assign(T, std::vector<int>(N + 1, 1));
   const size_t mark0 = B.mark();
   for (size_t i = 0; i < T; ++i) {
     const int t = tts[i];
     size_t mx = 1;
-    for (int k = 1; k < N; ++k) mx = std::max(mx, (size_t)((long long)rho[i][k] * x->dims[k] * x->rk(t, k + 1)));
+    for (int k = 0; k < N; ++k)
+      mx = std::max(mx, (size_t)((long long)rho[i][k] * x->dims[k] * x->rk(t, k + 1)));
     Y[i] = B.wd(mx);
     Yn[i] = B.wd(mx);
   }
+  // unit vectors of core k's completion in the rows of y_k that are zero (left index >= e):
+  // columns col0 .. col0 + cnt - 1, rows taken left index fastest
+  auto outside_units = [&](std::vector<CopyDesc>& v, double* core, int e_, int rh, int n, int yc, long long col0,
+                           long long cnt) {
+    const long long per = rh - e_;
+    if (cnt <= 0 || per <= 0) return;
+    const long long full = cnt / per, rem = cnt % per;
+    const long long cs = (long long)yc * n;          // column stride of the core's left unfolding
+    CopyDesc c{};
+    c.src = B.ctx->d_one;
+    c.alpha = 1.0;
+    c.ext[2] = c.ext[3] = 1;
+    if (full > 0) {
+      c.dst = core + e_ + cs * col0;
+      c.ext[0] = per; c.ext[1] = full;
+      c.ds[0] = 1 + cs; c.ds[1] = yc + cs * per;
+      v.push_back(c);
+    }
+    if (rem > 0) {
+      c.dst = core + e_ + (long long)yc * full + cs * (col0 + full * per);
+      c.ext[0] = rem; c.ext[1] = 1;
+      c.ds[0] = 1 + cs; c.ds[1] = 0;
+      v.push_back(c);
+    }
+  };
   for (int k = 0; k + 1 < N; ++k) {
     const size_t mk = B.mark();
+    std::vector<CopyDesc> cp0, cpQ, cpC;
+    std::vector<QRDesc> qrY, qrZ;
     std::vector<GemmDesc> gz, gp, gy;
-    std::vector<QRDesc> qr;
-    std::vector<CopyDesc> cp;
+    std::vector<ZeroDesc> zb;
+    std::vector<QApplyDesc> qa;
     const int n = (int)x->dims[k], nn = (int)x->dims[k + 1];
     const int s = sp.s[k + 1];
     const double wscale = 1.0 / std::sqrt((double)sp.p[k + 1]);
     for (size_t i = 0; i < T; ++i) {
       const int t = tts[i];
-      const int rh = rho[i][k], rhn = rho[i][k + 1], r1 = x->rk(t, k + 1), r2 = x->rk(t, k + 2);
-      // y_k: (rh, n, r1); for k = 0 it is core 0 of x (cap_0 = 1)
-      const double* Yk = (k == 0) ? x->core(t, 0) : Y[i];
-      const long long yk_ld = (k == 0) ? (long long)x->capr(t, 0) * n : (long long)rh * n;
-      double* Z = B.wd((size_t)rh * n * s);
+      const int rh = rho[i][k], rhn = rho[i][k + 1], c = x->rk(t, k + 1), r2 = x->rk(t, k + 2);
+      const int m = n * e[i];
+      const int q = std::min(std::min(m, c), s);
       const int yc = y->capr(t, k);
-      // Q goes straight into core k when the core's capacity equals its rank (same layout)
-      const bool direct = (yc == rh);
-      double* Q = direct ? y->core(t, k) : B.wd((size_t)rh * n * rhn);
-      double* P = B.wd((size_t)rhn * r1);
-      double* Tws = B.wd(qr_tws(rh * n, s));
-      gz.push_back(gd(rh * n, s, r1, Yk, 1, yk_ld, W[i][k + 1], 1, r1, Z, 1, (long long)rh * n, wscale));
-      qr.push_back({rh * n, s, Z, rh * n, Q, rh * n, nullptr, 0, Tws});
-      if (!direct)
-        cp.push_back(cd3(Q, y->core(t, k), rh, n, rhn, 1, rh, (long long)rh * n, 1, yc, (long long)yc * n));
-      gp.push_back(gd(rhn, r1, rh * n, Q, (long long)rh * n, 1, Yk, 1, yk_ld, P, 1, rhn));
-      gy.push_back(gd(rhn, nn * r2, r1, P, 1, rhn, x->core(t, k + 1), 1, x->capr(t, k + 1), Yn[i], 1, rhn));
+      double* core = y->core(t, k);
+      // Y: m x c with leading dimension m (k = 0: core 0 of x, whose left capacity is 1)
+      const double* Yk = (k == 0) ? x->core(t, 0) : Y[i];
+      const long long yld = (k == 0) ? (long long)x->capr(t, 0) * n : m;
+      const double* Wk = W[i][k + 1];                 // r_{k+1} x s, leading dimension r_{k+1}
+      double* P = B.wd((size_t)q * c);                 // Q^T y_k, its q nonzero rows
+      if (q == s) {                                    // F
+        double* Z = B.wd((size_t)m * s);
+        double* Q = B.wd((size_t)m * s);
+        double* Tws = B.wd(qr_tws(m, s));
+        gz.push_back(gd(m, s, c, Yk, 1, yld, Wk, 1, c, Z, 1, m, wscale));
+        qrZ.push_back({m, s, Z, m, Q, m, nullptr, 0, Tws});
+        cpC.push_back(cd3(Q, core, e[i], n, s, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
+        gp.push_back(gd(s, c, m, Q, m, 1, Yk, 1, yld, P, 1, s));
+      } else if (q == c) {                             // T: c < m, c < s
+        double* Yw = const_cast<double*>(Yk);
+        if (k == 0) {                                  // the QR overwrites its input: not x's core
+          Yw = B.wd((size_t)m * c);
+          cp0.push_back(cd2(Yk, Yw, m, c, 1, yld, 1, m));
+        }
+        double* R1 = B.wd((size_t)c * c);
+        double* M1 = B.wd((size_t)c * c);
+        double* QM = B.wd((size_t)c * c);
+        double* TwsY = B.wd(qr_tws(m, c));
+        double* TwsM = B.wd(qr_tws(c, c));
+        const int ncols = complete ? std::min(m, rhn) : c;
+        double* Bq = B.wd((size_t)m * ncols);
+        qrY.push_back({m, c, Yw, m, nullptr, 0, R1, c, TwsY});
+        gz.push_back(gd(c, c, c, R1, 1, c, Wk, 1, c, M1, 1, c, wscale));
+        qrZ.push_back({c, c, M1, c, QM, c, nullptr, 0, TwsM});
+        zb.push_back({Bq, (long long)m * ncols});
+        cpQ.push_back(cd2(QM, Bq, c, c, 1, c, 1, m));
+        if (ncols > c) {                               // unit vectors e_c .. e_{ncols-1}
+          CopyDesc u{};
+          u.src = B.ctx->d_one; u.dst = Bq + c + (long long)m * c; u.alpha = 1.0;
+          u.ext[0] = ncols - c; u.ext[1] = u.ext[2] = u.ext[3] = 1;
+          u.ds[0] = (long long)m + 1;
+          cpQ.push_back(u);
+        }
+        qa.push_back({m, c, Yw, m, TwsY, Bq, m, ncols, nullptr, nullptr, 0});
+        cpC.push_back(cd3(Bq, core, e[i], n, ncols, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
+        if (complete) outside_units(cpC, core, e[i], rh, n, yc, ncols, (long long)rhn - ncols);
+        gp.push_back(gd(c, c, c, QM, c, 1, R1, 1, c, P, 1, c));
+      } else {                                         // W: q = m <= c, m < s
+        double* M1 = B.wd((size_t)m * m);
+        double* QM = B.wd((size_t)m * m);
+        double* TwsM = B.wd(qr_tws(m, m));
+        gz.push_back(gd(m, m, c, Yk, 1, yld, Wk, 1, c, M1, 1, m, wscale));
+        qrZ.push_back({m, m, M1, m, QM, m, nullptr, 0, TwsM});
+        cpC.push_back(cd3(QM, core, e[i], n, m, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
+        if (complete) outside_units(cpC, core, e[i], rh, n, yc, m, (long long)rhn - m);
+        gp.push_back(gd(m, c, m, QM, m, 1, Yk, 1, yld, P, 1, m));
+      }
+      // y_{k+1} = P A_{k+1}: (q, nn, r_{k+2}) compact
+      gy.push_back(gd(q, nn * r2, c, P, 1, q, x->core(t, k + 1), 1, x->capr(t, k + 1), Yn[i], 1, q));
+      e[i] = q;
+      if (eff) (*eff)[i][k + 1] = q;
     }
+    B.copy(cp0);
+    B.qr(qrY);
     B.gemm(gz);
-    B.qr(qr);
-    B.copy(cp);
+    B.qr(qrZ);
+    B.zero(zb);
+    B.copy(cpQ);
+    B.qapply(qa);
+    B.copy(cpC);
     B.gemm(gp);
     B.gemm(gy);
     std::swap(Y, Yn);
@@ -460,9 +559,9 @@ void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<i
   std::vector<CopyDesc> cp;
   for (size_t i = 0; i < T; ++i) {
     const int t = tts[i];
-    const int rh = rho[i][N - 1], n = (int)x->dims[N - 1], yc = y->capr(t, N - 1);
+    const int n = (int)x->dims[N - 1], yc = y->capr(t, N - 1);
     const double* src = (N == 1) ? x->core(t, 0) : Y[i];
-    cp.push_back(cd2(src, y->core(t, N - 1), rh, n, 1, rh, 1, yc));
+    cp.push_back(cd2(src, y->core(t, N - 1), e[i], n, 1, e[i], 1, yc));
   }
   B.copy(cp);
   B.release(mark0);
@@ -517,11 +616,12 @@ void round_rand(ttc_context* c, ttc_batch* x, const std::vector<long long>& rks,
     if (tensor_core_sketch(o.precision)) emit_sketch_bf16(B, x, all, sp, S, W, o.precision == TTC_PREC_TF32);
     else emit_sketch_f64(B, x, all, sp, S, W);
     B.stage(1);
-    emit_rand_sweep(B, x, y, all, sp, W, rho_all);
+    std::vector<std::vector<int>> eff;
+    emit_rand_sweep(B, x, y, all, sp, W, rho_all, after == nullptr, &eff);
     B.stage(2);
     if (after) {
       emit_zero_check(B, y, all, N - 1, after->tol);
-      emit_svd_left(B, y, all, rho_all, after->tol, after->rmax);
+      emit_svd_left(B, y, all, eff, after->tol, after->rmax);
       emit_finalize(B, y, all, rho_all);
     }
     B.stage(3);

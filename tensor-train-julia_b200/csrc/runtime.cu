@@ -89,7 +89,9 @@ static void launch_op(ttc_context* c, const Plan& p, const Op& op) {
       case OP_GEMM: launch_gemm_f64((const GemmDesc*)d, op.count, op.total, s); break;
       case OP_QR: launch_qr((const QRDesc*)d, op.count, op.a, s, c->d_flags); break;
       case OP_QAPPLY: launch_qr_apply((const QApplyDesc*)d, op.count, op.a, s); break;
-      case OP_JACOBI: launch_jacobi((const JacobiDesc*)d, op.count, op.a, op.b, op.total != 0, s, c->d_flags, op.iw); break;
+      case OP_JACOBI:
+        launch_jacobi((const JacobiDesc*)d, op.count, op.a, op.b, op.total != 0, s, c->d_flags, op.iw, (int)op.rmax);
+        break;
       case OP_TRUNC: launch_truncate((const TruncDesc*)d, op.count, op.tol, op.rmax, s); break;
       case OP_SELECT: launch_select((const SelectDesc*)d, op.count, op.a, op.b, s); break;
       case OP_COPY: launch_copy((const CopyDesc*)d, op.count, op.total, s); break;
@@ -412,6 +414,7 @@ void Builder::jacobi(const std::vector<JacobiDesc>& v) {
     TTC_REQUIRE(2LL * 1 * (d.m + (d.W ? d.n : 0)) <= 25600 && d.n <= 25600, TTC_EDIM, "jacobi: matrix too large");
   }
   Op op; op.kind = OP_JACOBI; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm; op.b = nn;
+  op.rmax = ctx->jacobi_max_sweeps;              // the sweep cap (plans are rebuilt when it changes)
   op.iw = (int)v.size() <= kJacobiOrderMax ? wi(v.size()) : nullptr;   // largest problems first
   for (auto& d : v) op.total |= (d.W != nullptr);
   for (auto& d : v) op.flops += jacobi_flops(d.m, d.n);

@@ -99,6 +99,7 @@ struct ttc_context {
   double* d_sk = nullptr;           // host-provided sketch blocks
   size_t sk_cap = 0;
   bool profiling = false;           // per-kernel-family event timing (ttc_set_profiling)
+  int jacobi_max_sweeps = ttc::kJacobiDefaultSweeps;   // sweep cap of the one-sided Jacobi SVD
 };
 
 struct ttc_batch {

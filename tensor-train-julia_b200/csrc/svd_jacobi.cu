@@ -46,7 +46,7 @@ namespace ttc {
 namespace {
 constexpr int NT = 256;
 constexpr int NW = NT / 32;
-constexpr int MAX_SWEEPS = 40;
+
 // Rotation threshold |a_i.a_j| > tol * ||a_i|| ||a_j|| with tol = max(m, 16) eps, the worst-case
 // rounding error of an m-term FP64 dot product.  A threshold nearer the typical error
 // (sqrt(m) eps) is crossed by noise alone on a few of the ~m^2/2 pairs of every sweep when m is
@@ -347,7 +347,7 @@ __host__ __device__ __forceinline__ size_t dyn_doubles(int bw, int ms, int n, bo
 template <int RMAX>
 __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
     jacobi_svd_kernel(const JacobiDesc* __restrict__ descs, const int* __restrict__ order, int bw, int csize,
-                      int* flags) {
+                      int* flags, int max_sweeps) {
   extern __shared__ double sm[];
   __shared__ int s_any, s_nact;
   __shared__ double s_red[NW];
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   int* any0 = cluster.map_shared_rank(&s_any, 0);
   bool converged = false;
   int sweep = 0;
-  for (; sweep < MAX_SWEEPS && !converged; ++sweep) {
+  for (; sweep < max_sweeps && !converged; ++sweep) {
     bool any = false;
     const bool screen = (sweep >= 3) && (bw == 16);   // late sweeps: skip block pairs that need no rotation
     // (a) pairs inside each block; blocks dealt to the CTAs of the cluster
@@ -497,11 +497,13 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
     if (lane == 0) { sig[c] = sqrt(a); D.sigma[c] = sqrt(a); }
   }
   __syncthreads();
+  // the keys order NaN (a non-finite input, flagged by the QR) below every singular value, so
+  // that the ranks form a permutation whatever the values and perm stays a valid index list
   for (int c = tid; c < n; c += NT) {
-    const double v = sig[c];
+    const double v = (sig[c] == sig[c]) ? sig[c] : -1.0;
     int rank = 0;
     for (int j = 0; j < n; ++j) {
-      const double w = sig[j];
+      const double w = (sig[j] == sig[j]) ? sig[j] : -1.0;
       rank += (w > v) || (w == v && j < c);
     }
     D.perm[rank] = c;
@@ -566,7 +568,7 @@ static int jacobi_cluster_size(int count, int max_n, int bw, size_t smem, bool o
 
 template <int RMAX>
 static void launch_jacobi_t(const JacobiDesc* d_descs, int count, int max_n, int bw, size_t smem, cudaStream_t s,
-                            int* d_flags, int* order) {
+                            int* d_flags, int* order, int max_sweeps) {
   static PerDeviceOnce attr_once;
   int dev = 0;
   TTC_CUDA(cudaGetDevice(&dev));
@@ -590,19 +592,21 @@ static void launch_jacobi_t(const JacobiDesc* d_descs, int count, int max_n, int
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  TTC_CUDA(cudaLaunchKernelEx(&cfg, jacobi_svd_kernel<RMAX>, d_descs, (const int*)order, bw, csize, d_flags));
+  TTC_CUDA(cudaLaunchKernelEx(&cfg, jacobi_svd_kernel<RMAX>, d_descs, (const int*)order, bw, csize, d_flags,
+                              max_sweeps));
   TTC_CHECK_LAUNCH();
 }
 
 void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, bool accw, cudaStream_t s,
-                   int* d_flags, int* order) {
+                   int* d_flags, int* order, int max_sweeps) {
   if (count <= 0) return;
+  TTC_REQUIRE(max_sweeps >= 1, TTC_EARG, "jacobi: the sweep cap must be at least 1");
   size_t smem = 0;
   const int bw = jacobi_bw(max_m, max_n, accw, &smem);
   TTC_REQUIRE(smem <= 200 * 1024, TTC_EDIM, "jacobi: matrix too large for the shared-memory blocks");
   if (count > kJacobiOrderMax) order = nullptr;
-  if (max_m <= 256) launch_jacobi_t<8>(d_descs, count, max_n, bw, smem, s, d_flags, order);
-  else launch_jacobi_t<16>(d_descs, count, max_n, bw, smem, s, d_flags, order);
+  if (max_m <= 256) launch_jacobi_t<8>(d_descs, count, max_n, bw, smem, s, d_flags, order, max_sweeps);
+  else launch_jacobi_t<16>(d_descs, count, max_n, bw, smem, s, d_flags, order, max_sweeps);
 }
 
 }  // namespace ttc

@@ -51,6 +51,36 @@ void run_plan_once(ttc_context* c, const std::function<void(Builder&)>& fn) {
 
 extern "C" {
 
+// Sets the context's Jacobi SVD sweep cap (default 40), so that the tests can make the sweep run
+// out of sweeps (TTC_ENOCONV) on purpose and watch the retry.
+int ttc_test_set_jacobi_max_sweeps(ttc_context* c, int sweeps) {
+  try {
+    set_jacobi_max_sweeps(c, sweeps);
+    return TTC_OK;
+  } catch (const Error& e) {
+    c->err = e.what();
+    return e.status;
+  }
+}
+
+// Builds a plan whose copy descriptor points `offset` bytes past the end of the context's
+// workspace: the host-side registry check refuses it (TTC_EINTERNAL) before any launch.
+int ttc_test_bad_descriptor(ttc_context* c, long long offset) {
+  return hook(c, [&] {
+    ensure_workspace(c, 1 << 20);
+    double* past = reinterpret_cast<double*>(c->ws + c->ws_bytes + offset);
+    // the address must lie outside every registered allocation, or the plan below would run
+    bool registered = true;
+    try {
+      region_check(past, 4 * sizeof(double), "probe");
+    } catch (const Error&) {
+      registered = false;
+    }
+    TTC_REQUIRE(!registered, TTC_EARG, "test address lies inside a registered allocation");
+    run_plan_once(c, [&](Builder& B) { B.copy({cd2(past, past, 4, 1, 1, 4, 1, 4)}); });
+  });
+}
+
 // C = alpha * A * B + beta * C with split strides (a_str = {i0, i1, k0, k1, b}, ...).
 int ttc_test_gemm(ttc_context* c, int m, int n, int k, int batch, int m0, int n0, int k0e, const double* A,
                   long long a_len, const long long* as, const double* Bh, long long b_len, const long long* bs,

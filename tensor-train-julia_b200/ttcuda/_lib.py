@@ -41,7 +41,7 @@ class Stats(C.Structure):
     _fields_ = [("total_ms", f64), ("sketch_ms", f64), ("orth_ms", f64), ("svd_ms", f64), ("h2d_ms", f64),
                 ("d2h_ms", f64), ("kernel_launches", i64), ("kind_ms", f64 * 8), ("kind_launches", i64 * 8),
                 ("kind_flops", f64 * 8), ("jacobi_problems", i64), ("jacobi_sweeps_sum", i64),
-                ("jacobi_sweeps_max", i64), ("plans_built", i64)]
+                ("jacobi_sweeps_max", i64), ("plans_built", i64), ("svd_retries", i64)]
 
 
 KERNEL_KINDS = ["gemm_f64", "householder_qr", "jacobi_svd", "gemm_bf16_tcgen05", "mpo_apply", "other"]
