@@ -214,6 +214,130 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------- the other configurations
+def rand_cores(dims, ranks, g, normalise=False):
+    """N(0,1) cores of the given (clamped) ranks, Julia layout (n, r_{k-1}, r_k); with `normalise`
+    each core is scaled by 1/sqrt(n r_k) like rand_tt(...; normalise=true)."""
+    out = []
+    for k, n in enumerate(dims):
+        c = g.standard_normal((n, ranks[k], ranks[k + 1]))
+        if normalise:
+            c /= math.sqrt(n * ranks[k + 1])
+        out.append(np.asfortranarray(c))
+    return out
+
+
+def device_ms(ctx, fn, reps):
+    """Device time of `reps` calls of fn (events on the library's stream), after one warm-up call."""
+    import torch
+    fn()
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st = torch.cuda.current_stream()
+    e0.record(st)
+    for _ in range(reps):
+        fn()
+    e1.record(st)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def other_configs(ttcuda, ctx, hbm_peak):
+    """Configs 1, 2 and 4 of the benchmark set, each through the library's public API on host
+    tensors (end to end, transfers included) and, where one kernel bounds it, with that kernel's
+    device time from the per-kernel profile."""
+    import ttcuda.models as tm
+    out = {}
+    # config 1: tt_rounding(X; tol=1e-8, rmax=64), X = sum_{j=1..8} 2^-j X_j, X_j rank 8, n=2, d=20
+    g = np.random.default_rng(101)
+    dims = (2,) * 20
+    r8 = r_and_d([1] + [8] * 19 + [1], dims, 8)
+    X = None
+    for j in range(1, 9):
+        t = ttcuda.tt_scale(2.0 ** -j, ttcuda.TTvector(20, rand_cores(dims, r8, g), dims, r8))
+        X = t if X is None else ttcuda.tt_add(X, t)
+    ms1 = device_ms(ctx, lambda: ttcuda.tt_rounding(X, tol=1e-8, rmax=64), 20)
+    xb = ttcuda.DeviceBatch.from_tts([X], ctx=ctx)
+    yb = ttcuda.DeviceBatch(dims, [X.ttv_rks], ctx=ctx)
+    ms1d = device_ms(ctx, lambda: xb.round_det(yb, tol=1e-8, rmax=64, sync=False), 50)
+    Y = yb.download()[0]
+    out["config1"] = {"workload": "tt_rounding(X; tol=1e-8, rmax=64), X = sum of 8 rank-8 N(0,1) TTs scaled 2^-j, "
+                                  "n=2, d=20 (input ranks up to 64)",
+                      "value": 1e3 / ms1, "unit": "roundings/s", "ms_per_rounding": ms1,
+                      "path": "ttc_tt_rounding on host tensors (upload, round, download)",
+                      "device_resident_ms": ms1d, "output_ranks_max": max(Y.ttv_rks)}
+    # config 2: 1D Hubbard MPO (16 sites, t=1, U=4) applied to a rank-128 TT; apply, and
+    # operator-aware randomized rounding with a rank-138 Gaussian sketch
+    h, V = tm.hubbard_1D(16, t=1.0, U=4.0)
+    H = tm.hV_to_mpo(h, V, (2,) * 32)
+    dims2 = (2,) * 32
+    r128 = r_and_d([1] + [128] * 31 + [1], dims2, 128)
+    y = ttcuda.TTvector(32, rand_cores(dims2, r128, np.random.default_rng(40), normalise=True), dims2, r128)
+    ctx.set_profiling(True)
+    Hy = ttcuda.mpo_apply(H, y)
+    prof = ctx.kernel_profile()["mpo_apply"]
+    ctx.set_profiling(False)
+    ms_apply = device_ms(ctx, lambda: ttcuda.mpo_apply(H, y), 5)
+    out_bytes = sum(8 * 2 * Hy.ttv_rks[k] * Hy.ttv_rks[k + 1] for k in range(32))
+    in_bytes = sum(8 * c.size for c in y.ttv_vec) + sum(8 * c.size for c in H.tto_vec)
+    kern_ms = prof[0] / max(1, prof[1]) * prof[1]      # device time of all apply launches of one call
+    gbs = (out_bytes + in_bytes) / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else None
+    rks = [1] + [138] * 31 + [1]
+    ms_op = device_ms(ctx, lambda: ttcuda.ttrand_rounding_op([1.0], H, [y], rks, orthogonal=False, seed=5,
+                                                             block_rks=138), 3)
+    ms_op_tf = device_ms(ctx, lambda: ttcuda.ttrand_rounding_op([1.0], H, [y], rks, orthogonal=False, seed=5,
+                                                                block_rks=138, precision="tf32"), 3)
+    z64 = ttcuda.ttrand_rounding_op([1.0], H, [y], rks, orthogonal=False, seed=5, block_rks=138)
+    ztf = ttcuda.ttrand_rounding_op([1.0], H, [y], rks, orthogonal=False, seed=5, block_rks=138, precision="tf32")
+    dz = ttcuda.tt_add(z64, ttcuda.tt_scale(-1.0, ztf))
+    rel_tf = ttcuda.norm(dz) / ttcuda.norm(z64)
+    out["config2"] = {"workload": "1D Hubbard MPO (hV_to_mpo on the GPU, 16 sites, t=1, U=4, MPO ranks up to "
+                                  f"{max(H.tto_rks)}) x rank-128 N(0,1) TT; sketch rank 138 (block_rks=138)",
+                      "apply": {"value": 1e3 / ms_apply, "unit": "contractions/s", "ms": ms_apply,
+                                "path": "ttc_mpo_apply on host tensors (output ranks up to "
+                                        f"{max(Hy.ttv_rks)}, {out_bytes / 1e6:.0f} MB written back)",
+                                "roofline": {"kernel": "apply_kernel", "bound": "hbm", "achieved": gbs,
+                                             "peak": hbm_peak, "unit": "GB/s",
+                                             "frac": (gbs / hbm_peak) if (gbs and hbm_peak) else None,
+                                             "bytes_per_call": out_bytes + in_bytes,
+                                             "launch_ms": kern_ms, "launches": prof[1]}},
+                      "operator_rounding_fp64": {"value": 1e3 / ms_op, "unit": "roundings/s", "ms": ms_op,
+                                                 "path": "ttc_ttrand_rounding_op (H y never formed), FP64"},
+                      "operator_rounding_tf32": {"value": 1e3 / ms_op_tf, "unit": "roundings/s", "ms": ms_op_tf,
+                                                 "path": "the same with the operator sketch on the tcgen05 tensor "
+                                                         "cores (TF32 operands, FP32 accumulation), FP64 range finder",
+                                                 "rel_diff_vs_fp64": rel_tf,
+                                                 "ranks_identical_fp64": ztf.ttv_rks == z64.ttv_rks}}
+    # config 4: gradient of <x|H|x>/<x|x>, 4x4 open Hubbard (U=8) in snake ordering, x rank 256
+    h4, V4 = tm.hubbard_2D(4, 4, t=1.0, U=8.0, w_pbc=False, L_pbc=False)
+    sg = tm.snake_order(4, 4)
+    H4 = tm.hV_to_mpo(h4[np.ix_(sg, sg)], V4[np.ix_(sg, sg, sg, sg)], (2,) * 32)
+    r256 = r_and_d([1] + [256] * 31 + [1], dims2, 256)
+    x4 = ttcuda.TTvector(32, rand_cores(dims2, r256, np.random.default_rng(41), normalise=True), dims2, r256)
+    ctx.set_profiling(True)
+    ttcuda.rayleigh_grad(H4, x4, ckpt_every=4)
+    prof4 = ctx.kernel_profile()["gemm_f64"]
+    ctx.set_profiling(False)
+    ms_g = device_ms(ctx, lambda: ttcuda.rayleigh_grad(H4, x4, ckpt_every=4), 3)
+    ms_g32 = device_ms(ctx, lambda: ttcuda.rayleigh_grad(H4, x4, ckpt_every=4, precision="fp32"), 3)
+    R64, G64 = ttcuda.rayleigh_grad(H4, x4, ckpt_every=4)
+    R32, G32 = ttcuda.rayleigh_grad(H4, x4, ckpt_every=4, precision="fp32")
+    gd = math.sqrt(sum(float(np.sum((a - b) ** 2)) for a, b in zip(G32, G64)))
+    gn = math.sqrt(sum(float(np.sum(b ** 2)) for b in G64))
+    out["config4"] = {"workload": "gradient of <x|H|x>/<x|x> w.r.t. every core, 4x4 open Hubbard MPO (t=1, U=8, "
+                                  f"snake ordering, MPO ranks up to {max(H4.tto_rks)}), x rank 256, environments "
+                                  "checkpointed every 4 sites, FP64",
+                      "value": 1e3 / ms_g, "unit": "gradients/s", "ms": ms_g,
+                      "path": "ttc_rayleigh_grad on host tensors",
+                      "gemm_f64": {"ms": prof4[0], "launches": prof4[1], "gflop": prof4[2] / 1e9,
+                                   "tflops": (prof4[2] / (prof4[0] / 1e3) / 1e12) if prof4[0] > 0 else None},
+                      "fp32": {"value": 1e3 / ms_g32, "unit": "gradients/s", "ms": ms_g32,
+                               "variant": "FP32 cores and environments, FP32 accumulation",
+                               "rel_diff_gradient_vs_fp64": gd / gn, "rel_diff_value_vs_fp64": abs(R32 - R64) / abs(R64)}}
+    return out
+
+
 # ---------------------------------------------------------------------------- ours
 def main():
     ap = argparse.ArgumentParser()
@@ -223,6 +347,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-configs", action="store_true", help="skip the config 1, 2 and 4 lines")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -383,6 +508,17 @@ def main():
     flops_mixed = sum(v[2] for v in prof_m.values())
     flops_fp64 = sum(v[2] for v in prof_f.values())
 
+    others = None
+    if rank == 0 and not args.no_other_configs:
+        hbm, hbm_src = 6650.0, "fallback (MEASURED_PEAKS.json absent)"
+        try:
+            hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+            hbm_src = "MEASURED_PEAKS.json hbm_gbs (measured)"
+        except Exception:
+            pass
+        others = other_configs(ttcuda, ctx, hbm)
+        others["config2"]["apply"]["roofline"]["peak_source"] = hbm_src
+
     # end-to-end through the C ABI with host buffers (upload, round, download) every step; device
     # events on the library's stream bracket the whole loop, host-side gaps included.  The
     # inputs sit in page-locked host memory (copied there before the timed region), the results
@@ -469,6 +605,8 @@ def main():
             line["cpu_baseline"] = cpu
         if oracle_cmp:
             line["accuracy"].update(oracle_cmp)
+        if others:
+            line["configs"] = others
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

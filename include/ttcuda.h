@@ -38,7 +38,8 @@ typedef enum {
 } ttc_status;
 
 enum { TTC_DIR_LEFT = 0, TTC_DIR_RIGHT = 1 };         /* direction=:left / :right      */
-enum { TTC_PREC_FP64 = 0, TTC_PREC_BF16 = 1, TTC_PREC_TF32 = 2 };   /* sketch-contraction precision */
+enum { TTC_PREC_FP64 = 0, TTC_PREC_BF16 = 1, TTC_PREC_TF32 = 2,   /* sketch-contraction precision */
+       TTC_PREC_FP32 = 3 };                                         /* FP32 with FP32 accumulation (gradient) */
 
 typedef struct ttc_context ttc_context;
 typedef struct ttc_batch ttc_batch;
@@ -259,6 +260,11 @@ int ttc_tt_scale(ttc_context* ctx, double a, const ttc_ttv* x, ttc_ttv_out* out)
  * the others (memory O(d/ckpt) environments instead of O(d)). */
 int ttc_rayleigh_grad(ttc_context* ctx, const ttc_tto* H, const ttc_ttv* x, int32_t ckpt_every,
                       double* value, double* const* grads);
+/* The same gradient with every contraction in a chosen precision: TTC_PREC_FP64, or TTC_PREC_FP32
+ * (FP32 cores and environments, FP32 accumulation; value and gradient are returned widened to
+ * double).  No reference method either. */
+int ttc_rayleigh_grad_prec(ttc_context* ctx, const ttc_tto* H, const ttc_ttv* x, int32_t ckpt_every,
+                           int32_t precision, double* value, double* const* grads);
 
 /* Householder QR of one m x n matrix in device memory that allocates nothing.
  * No counterpart in the reference (the Julia package calls LAPACK qr on host arrays).  It

@@ -77,6 +77,6 @@ double dot_operator_host(ttc_context* c, const ttc_ttv* psi, const ttc_tto* H, c
 void tt_add_host(ttc_context* c, const ttc_ttv* x, const ttc_ttv* y, ttc_ttv_out* out);
 void tt_scale_host(ttc_context* c, double a, const ttc_ttv* x, ttc_ttv_out* out);
 void rayleigh_grad_host(ttc_context* c, const ttc_tto* H, const ttc_ttv* x, int ckpt, double* value,
-                        double* const* grads);
+                        double* const* grads, bool f32 = false);
 
 }  // namespace ttc

@@ -27,6 +27,11 @@ struct Builder {
   int* diag_ints(int n);
 
   void gemm(std::vector<GemmDesc> v);
+  // the same problems with float data (FP32 accumulation)
+  void gemm32(std::vector<GemmDesc> v);
+  // FP64 -> FP32 (nearest) and FP32 -> FP64 conversions with the CvtDesc index map
+  void cvt_f32(const std::vector<CvtDesc>& v);
+  void widen(const std::vector<CvtDesc>& v);
   void qr(const std::vector<QRDesc>& v);
   void qapply(const std::vector<QApplyDesc>& v);
   void jacobi(const std::vector<JacobiDesc>& v);

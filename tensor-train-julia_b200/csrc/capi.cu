@@ -711,4 +711,14 @@ int ttc_rayleigh_grad(ttc_context* c, const ttc_tto* H, const ttc_ttv* x, int32_
   return guard(c, [&] { rayleigh_grad_host(c, H, x, ckpt_every, value, grads); });
 }
 
+int ttc_rayleigh_grad_prec(ttc_context* c, const ttc_tto* H, const ttc_ttv* x, int32_t ckpt_every, int32_t precision,
+                           double* value, double* const* grads) {
+  if (!c || !H || !x || !value || !grads) return TTC_EARG;
+  return guard(c, [&] {
+    TTC_REQUIRE(precision == TTC_PREC_FP64 || precision == TTC_PREC_FP32, TTC_EARG,
+                "rayleigh_grad: precision must be TTC_PREC_FP64 or TTC_PREC_FP32");
+    rayleigh_grad_host(c, H, x, ckpt_every, value, grads, precision == TTC_PREC_FP32);
+  });
+}
+
 }  // extern "C"

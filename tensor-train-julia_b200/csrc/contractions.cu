@@ -90,7 +90,7 @@ struct OpEnvStep {
   int batch; long long v_b, s_b, w_b;  // block batching (sketch blocks)
 };
 
-static void emit_op_env(Builder& B, const std::vector<OpEnvStep>& steps) {
+static void emit_op_env(Builder& B, const std::vector<OpEnvStep>& steps, bool f32 = false) {
   std::vector<GemmDesc> g1, g2, g3;
   for (const auto& st : steps) {
     const int r = st.r, r1 = st.r1, R = st.R, R1 = st.R1, n = st.n, g = st.g;
@@ -117,9 +117,15 @@ static void emit_op_env(Builder& B, const std::vector<OpEnvStep>& steps) {
     d3.batch = st.batch; d3.a_b = (long long)r * R * n * g; d3.b_b = st.s_b; d3.c_b = st.w_b;
     g3.push_back(d3);
   }
-  B.gemm(g1);
-  B.gemm(g2);
-  B.gemm(g3);
+  if (f32) {
+    B.gemm32(g1);
+    B.gemm32(g2);
+    B.gemm32(g3);
+  } else {
+    B.gemm(g1);
+    B.gemm(g2);
+    B.gemm(g3);
+  }
 }
 
 void emit_sketch_op_f64(Builder& B, const DevTTO& H, ttc_batch* x, int t, const SketchPlan& sp,
@@ -143,6 +149,126 @@ void emit_sketch_op_f64(Builder& B, const DevTTO& H, ttc_batch* x, int t, const 
     st.s_b = (long long)st.n * st.g * st.cdim;
     st.w_b = (long long)st.r * st.R * st.cdim;
     emit_op_env(B, {st});
+    B.release(mk);
+  }
+}
+
+// The operator sketch on the tcgen05 tensor cores (BF16 operands, or FP32 operands read as
+// TF32), FP32 accumulation: per site and block, the three contractions of
+// contract_sketch_core_backwards!(W, A, B, S, V) (src/sketches.jl:1648-1713) as three GEMMs,
+//   G1  T1[(a,z), (be,ga)] = sum_al A[a,z,al] V[al,(be,ga)]
+//   G2  T2[(a,ga), (b,ze)] = sum_{(z,be)} T1[a,z,be,ga] H[b,ze,z,be]
+//   G3  W[(a,b), c]        = sum_{(ze,ga)} T2[a,b,ze,ga] S[(ze,ga), c]
+// each epilogue writing the next GEMM's K-major operand directly (split row and column strides),
+// G3 also W in FP64 (for the FP64 range finder) and the next site's V operand.  Operands are
+// zero-padded to 16-byte rows; the TT core, the MPO core and the sketch blocks are converted
+// once per call.
+static inline long long pad_k(long long v, bool tf32) { const long long c = tf32 ? 4 : 8; return (v + c - 1) / c * c; }
+
+void emit_sketch_op_tc(Builder& B, const DevTTO& H, ttc_batch* x, int t, const SketchPlan& sp,
+                       const std::vector<double*>& S, std::vector<double*>& W, bool tf32) {
+  const int N = x->N;
+  const long long esz = tf32 ? 4 : 2;
+  W.assign(N + 1, nullptr);
+  std::vector<ZeroDesc> zr;
+  auto buf = [&](long long elems) -> void* {
+    const long long nd = (elems * esz + 7) / 8;
+    double* p = B.wd((size_t)nd);
+    zr.push_back({p, nd});
+    return (void*)p;
+  };
+  auto at = [&](const void* p, long long elems) -> void* { return (void*)((const char*)p + elems * esz); };
+  std::vector<void*> A16(N), H16(N), S16(N), V16(N + 1);
+  std::vector<long long> ldv(N + 1);
+  std::vector<CvtDesc> cv;
+  for (int k = 0; k < N; ++k) {
+    const long long n = x->dims[k], r = x->rk(t, k), r1 = x->rk(t, k + 1), xc = x->capr(t, k);
+    const long long R = H.rks[k], R1 = H.rks[k + 1], g = sp.b[k + 1], cd = sp.b[k], pk = sp.p[k];
+    W[k] = B.wd((size_t)(r * R * cd * pk));
+    ldv[k] = pad_k(r, tf32);
+    V16[k] = (k > 0) ? buf(ldv[k] * R * cd * pk) : nullptr;
+    // A16: row (a + r z), K = al
+    const long long lda = pad_k(r1, tf32);
+    A16[k] = buf(r * n * lda);
+    for (long long z = 0; z < n; ++z) {
+      CvtDesc c{};
+      c.src = x->core(t, k) + z * xc; c.dst = at(A16[k], r * z * lda);
+      c.rows = r; c.cols = r1; c.ss_i = 1; c.ss_j = xc * n; c.ds_i = lda; c.ds_j = 1; c.alpha = 1.0;
+      cv.push_back(c);
+    }
+    // H16: row (b + R ze), K = (z + n be); internal H (b, ze, z, be) at b + R (ze + n (z + n be))
+    const long long ldh = pad_k(n * R1, tf32);
+    H16[k] = buf(R * n * ldh);
+    {
+      CvtDesc c{};
+      c.src = H.core(k); c.dst = H16[k];
+      c.rows = R * n; c.cols = n * R1; c.ss_i = 1; c.ss_j = R * n; c.ds_i = ldh; c.ds_j = 1; c.alpha = 1.0;
+      cv.push_back(c);
+    }
+    // S16: row c, K = (ze + n ga); block j of S at S[k] + j n g cd
+    const long long lds = pad_k(n * g, tf32);
+    S16[k] = buf(lds * cd * pk);
+    for (long long j = 0; j < pk; ++j) {
+      CvtDesc c{};
+      c.src = S[k] + j * n * g * cd; c.dst = at(S16[k], j * lds * cd);
+      c.rows = n * g; c.cols = cd; c.ss_i = 1; c.ss_j = n * g; c.ds_i = 1; c.ds_j = lds; c.alpha = 1.0;
+      cv.push_back(c);
+    }
+  }
+  W[N] = B.ctx->d_one;
+  ldv[N] = pad_k(1, tf32);
+  V16[N] = buf(ldv[N]);
+  {
+    CvtDesc one{};
+    one.src = B.ctx->d_one; one.dst = V16[N];
+    one.rows = 1; one.cols = 1; one.ss_i = 0; one.ss_j = 0; one.ds_i = 1; one.ds_j = 1; one.alpha = 1.0;
+    cv.push_back(one);
+  }
+  B.zero(zr);
+  B.cvt_bf16(cv, tf32);
+  for (int k = N - 1; k >= 0; --k) {
+    const size_t mk = B.mark();
+    zr.clear();
+    std::vector<Bf16GemmDesc> g1, g2, g3;
+    const long long n = x->dims[k], r = x->rk(t, k), r1 = x->rk(t, k + 1);
+    const long long R = H.rks[k], R1 = H.rks[k + 1], g = sp.b[k + 1], cd = sp.b[k], pk = sp.p[k];
+    const long long ldt1 = pad_k(n * R1, tf32), ldt2 = pad_k(n * g, tf32), lda = pad_k(r1, tf32);
+    const long long lds = pad_k(n * g, tf32), ldh = pad_k(n * R1, tf32);
+    for (long long j = 0; j < pk; ++j) {
+      void* T1 = buf(r * g * ldt1);
+      void* T2 = buf(r * R * ldt2);
+      const long long jn = (k < N - 1) ? j : 0;     // W_N is the single constant block
+      Bf16GemmDesc d1{};
+      d1.m = (int)(r * n); d1.n = (int)(R1 * g); d1.k = (int)r1; d1.m0 = (int)r;
+      d1.A = A16[k]; d1.lda = lda;
+      d1.B = at(V16[k + 1], jn * ldv[k + 1] * R1 * g); d1.ldb = ldv[k + 1];
+      d1.C16 = T1; d1.h_i0 = ldt1; d1.h_i1 = 1;                  // row (a + r ga), K (z + n be)
+      d1.n0 = (int)R1; d1.h_j = n; d1.h_j1 = r * ldt1;
+      d1.alpha = 1.0;
+      g1.push_back(d1);
+      Bf16GemmDesc d2{};
+      d2.m = (int)(r * g); d2.n = (int)(R * n); d2.k = (int)(n * R1); d2.m0 = (int)r;
+      d2.A = T1; d2.lda = ldt1;
+      d2.B = H16[k]; d2.ldb = ldh;
+      d2.C16 = T2; d2.h_i0 = ldt2; d2.h_i1 = n;                  // row (a + r b), K (ze + n ga)
+      d2.n0 = (int)R; d2.h_j = r * ldt2; d2.h_j1 = 1;
+      d2.alpha = 1.0;
+      g2.push_back(d2);
+      Bf16GemmDesc d3{};
+      d3.m = (int)(r * R); d3.n = (int)cd; d3.k = (int)(n * g); d3.m0 = (int)r;
+      d3.A = T2; d3.lda = ldt2;
+      d3.B = at(S16[k], j * lds * cd); d3.ldb = lds;
+      d3.C64 = W[k] + j * r * R * cd; d3.c_i0 = 1; d3.c_i1 = r; d3.c_j = r * R;
+      if (k > 0) {                                               // next site's V: (a, b, c) at a + ldv (b + R c)
+        d3.C16 = at(V16[k], j * ldv[k] * R * cd); d3.h_i0 = 1; d3.h_i1 = ldv[k]; d3.h_j = ldv[k] * R;
+      }
+      d3.alpha = 1.0;
+      g3.push_back(d3);
+    }
+    B.zero(zr);
+    B.bf16gemm(g1, tf32);
+    B.bf16gemm(g2, tf32);
+    B.bf16gemm(g3, tf32);
     B.release(mk);
   }
 }
@@ -202,7 +328,10 @@ void rand_rounding_general(ttc_context* c, int m, const double* alpha, const ttc
       else emit_sketch_f64(B, X, tt_terms, sp, S, Wt);
       for (size_t i = 0; i < tt_terms.size(); ++i) W[tt_terms[i]] = Wt[i];
     }
-    if (op) emit_sketch_op_f64(B, *H, X, 0, sp, S, W[0]);
+    if (op) {
+      if (tensor_core_sketch(sk.precision)) emit_sketch_op_tc(B, *H, X, 0, sp, S, W[0], sk.precision == TTC_PREC_TF32);
+      else emit_sketch_op_f64(B, *H, X, 0, sp, S, W[0]);
+    }
     B.stage(1);
     // projected cores, ping-pong buffers per term
     std::vector<double*> Yc(m), Yn(m);
@@ -584,7 +713,7 @@ double norm_host(ttc_context* c, const ttc_ttv* x) {
 //   (Heff_k x_k)[a, i, d] = sum L_k[a,b,c] H_k[b,i,j,e] x_k[c,j,f] R_{k+1}[d,e,f].
 // Left environments are stored only every `ckpt` sites and recomputed segment by segment.
 void rayleigh_grad_host(ttc_context* c, const ttc_tto* Hh, const ttc_ttv* x, int ckpt, double* value,
-                        double* const* grads) {
+                        double* const* grads, bool f32) {
   BatchHolder BH;
   ttc_batch* X = BH.add(batch_from_host(c, x, nullptr));
   std::unique_ptr<DevTTO> H(tto_upload(c, Hh));
@@ -592,6 +721,53 @@ void rayleigh_grad_host(ttc_context* c, const ttc_tto* Hh, const ttc_ttv* x, int
   TTC_REQUIRE(H->N == N && H->dims == X->dims, TTC_EDIM, "rayleigh_grad: dimensions differ");
   TTC_REQUIRE(H->rks[N] == 1, TTC_EDIM, "rayleigh_grad: last operator rank must be 1");
   if (ckpt <= 0) ckpt = 1;
+  // FP32 variant: float copies of the TT and MPO cores (same element offsets), every contraction
+  // on the FP32 grouped GEMM, environments and gradient in float, widened for the host
+  const size_t esz = f32 ? sizeof(float) : sizeof(double);
+  float* Xf = nullptr;
+  float* Hf = nullptr;
+  std::vector<double*> own;
+  struct FreeV { std::vector<double*>& v; ~FreeV() { for (auto* p : v) { region_remove(p); cudaFree(p); } } } fv{own};
+  auto dev_alloc = [&](size_t bytes) {
+    double* p = nullptr;
+    TTC_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+    own.push_back(p);
+    region_add(p, std::max<size_t>(bytes, 16));
+    return p;
+  };
+  if (f32) {
+    size_t ht = 0;
+    for (int k = 0; k < N; ++k)
+      ht = std::max<size_t>(ht, (size_t)H->off[k] + (size_t)H->rks[k] * H->dims[k] * H->dims[k] * H->rks[k + 1]);
+    Xf = reinterpret_cast<float*>(dev_alloc(sizeof(float) * (size_t)X->total));
+    Hf = reinterpret_cast<float*>(dev_alloc(sizeof(float) * ht));
+    run_once(c, [&](Builder& B) {
+      CvtDesc a{}, h{};
+      a.src = X->d_cores; a.dst = Xf; a.rows = X->total; a.cols = 1; a.ss_i = 1; a.ds_i = 1; a.alpha = 1.0;
+      h.src = H->d; h.dst = Hf; h.rows = (long long)ht; h.cols = 1; h.ss_i = 1; h.ds_i = 1; h.alpha = 1.0;
+      B.cvt_f32({a, h});
+    });
+  }
+  auto xcore = [&](int k) -> double* {
+    return f32 ? reinterpret_cast<double*>(Xf + X->off[k]) : X->core(0, k);
+  };
+  auto hcore = [&](int k) -> double* {
+    return f32 ? reinterpret_cast<double*>(Hf + H->off[k]) : H->core(k);
+  };
+  auto GEMM = [&](Builder& B, std::vector<GemmDesc> v) {
+    if (f32) B.gemm32(std::move(v));
+    else B.gemm(std::move(v));
+  };
+  // 1.0 into the first element of a buffer of this precision
+  auto set_one = [&](Builder& B, double* dst) {
+    if (f32) {
+      CvtDesc o1{};
+      o1.src = B.ctx->d_one; o1.dst = dst; o1.rows = 1; o1.cols = 1; o1.ss_i = 1; o1.ds_i = 1; o1.alpha = 1.0;
+      B.cvt_f32({o1});
+    } else {
+      B.copy({cd2(B.ctx->d_one, dst, 1, 1, 0, 0, 0, 0)});
+    }
+  };
   auto rk = [&](int k) { return X->rk(0, k); };
   auto Rk = [&](int k) { return H->rks[k]; };
   // device buffers (outside the plan workspace): checkpoints, segment cache, right envs, grads
@@ -600,20 +776,16 @@ void rayleigh_grad_host(ttc_context* c, const ttc_tto* Hh, const ttc_ttv* x, int
   size_t gsz = 0;
   std::vector<size_t> goff(N);
   for (int k = 0; k < N; ++k) { goff[k] = gsz; gsz += (size_t)rk(k) * X->dims[k] * rk(k + 1); }
-  double* dG = nullptr;
-  TTC_CUDA(cudaMalloc(&dG, sizeof(double) * (gsz + 4)));
-  region_add(dG, sizeof(double) * (gsz + 4));
-  struct Free { double* p; ~Free() { if (p) { region_remove(p); cudaFree(p); } } } fg{dG};
-  double* dval = dG + gsz;   // [<x|H|x>, <x|x>]
+  double* dG = dev_alloc(esz * gsz);                  // gradient (this precision), offsets goff
+  double* dval = dev_alloc(sizeof(double) * 4);       // [<x|H|x>, <x|x>] in FP64
+  auto gcore = [&](int k) -> double* {
+    return f32 ? reinterpret_cast<double*>(reinterpret_cast<float*>(dG) + goff[k]) : dG + goff[k];
+  };
   // pass 1: left environments with checkpoints, value
   std::vector<double*> Lh_ck(N + 1, nullptr), Ln_ck(N + 1, nullptr);
-  std::vector<double*> own;
-  struct FreeV { std::vector<double*>& v; ~FreeV() { for (auto* p : v) { region_remove(p); cudaFree(p); } } } fv{own};
   for (int k = 0; k <= N; k += ckpt) {
-    double* a; double* b;
-    TTC_CUDA(cudaMalloc(&a, sizeof(double) * hsz[k])); own.push_back(a); region_add(a, sizeof(double) * hsz[k]);
-    TTC_CUDA(cudaMalloc(&b, sizeof(double) * nsz[k])); own.push_back(b); region_add(b, sizeof(double) * nsz[k]);
-    Lh_ck[k] = a; Ln_ck[k] = b;
+    Lh_ck[k] = dev_alloc(esz * hsz[k]);
+    Ln_ck[k] = dev_alloc(esz * nsz[k]);
   }
   // left env step k -> k+1 (bra = ket = x):  L'[a',b',c'] = sum L[a,b,c] x[a,i,a'] H[b,i,j,b'] x[c,j,c']
   // computed as the right-env contraction of the mirrored indices: W[c',b',a'] with A = x (ket), S = x (bra).
@@ -622,41 +794,42 @@ void rayleigh_grad_host(ttc_context* c, const ttc_tto* Hh, const ttc_ttv* x, int
     const int xc = X->capr(0, k);
     // T1[(a, b), (j, c')] = sum_c L[a,b,c] x[c, j, c']   (L as ((a,b) x c))
     double* T1 = B.wd((size_t)r0 * R0 * n * r1);
-    B.gemm({gd(r0 * R0, n * r1, r0, Lh, 1, (long long)r0 * R0, X->core(0, k), 1, xc, T1, 1, (long long)r0 * R0)});
+    GEMM(B, {gd(r0 * R0, n * r1, r0, Lh, 1, (long long)r0 * R0, xcore(k), 1, xc, T1, 1, (long long)r0 * R0)});
     double* T2 = B.wd((size_t)r0 * n * r1 * R1);
     // T2[(a, c'), (i, b')] = sum_{(b,j)} T1[a, b, j, c'] H[b, i, j, b']   (stored (a, i, c', b'))
     GemmDesc f{};
     f.m = r0 * r1; f.n = n * R1; f.k = R0 * n; f.batch = 1;
     f.m0 = r0; f.n0 = n; f.k0e = R0;
     f.A = T1; f.a_i0 = 1; f.a_i1 = (long long)r0 * R0 * n; f.a_k0 = r0; f.a_k1 = (long long)r0 * R0;
-    f.B = H->core(k); f.b_k0 = 1; f.b_k1 = (long long)R0 * n; f.b_j0 = R0; f.b_j1 = (long long)R0 * n * n;
+    f.B = hcore(k); f.b_k0 = 1; f.b_k1 = (long long)R0 * n; f.b_j0 = R0; f.b_j1 = (long long)R0 * n * n;
     // T2[(a, i), (c', b')] layout (a, i, c', b'): a -> 1, c' -> r0*n, i -> r0, b' -> r0*n*r1
     f.C = T2; f.c_i0 = 1; f.c_i1 = (long long)r0 * n; f.c_j0 = r0; f.c_j1 = (long long)r0 * n * r1;
     f.alpha = 1.0; f.beta = 0.0;
-    B.gemm({f});
+    GEMM(B, {f});
     // L'[a', (b', c')] = sum_{(a, i)} x[a, i, a'] T2[(a, i), (c', b')]  -> stored (a', b', c')
     GemmDesc h{};
     h.m = r1; h.n = r1 * R1; h.k = r0 * n; h.batch = 1;
     h.m0 = r1; h.n0 = r1; h.k0e = r0;
-    h.A = X->core(0, k); h.a_i0 = (long long)xc * n; h.a_i1 = 0; h.a_k0 = 1; h.a_k1 = xc;
+    h.A = xcore(k); h.a_i0 = (long long)xc * n; h.a_i1 = 0; h.a_k0 = 1; h.a_k1 = xc;
     h.B = T2; h.b_k0 = 1; h.b_k1 = r0; h.b_j0 = (long long)r0 * n; h.b_j1 = (long long)r0 * n * r1;
     h.C = Lh1; h.c_i0 = 1; h.c_i1 = 0; h.c_j0 = (long long)r1 * R1; h.c_j1 = r1;
     h.alpha = 1.0; h.beta = 0.0;
-    B.gemm({h});
+    GEMM(B, {h});
     // norm env: Ln'[a', c'] = sum x[a,i,a'] (sum_c Ln[a,c] x[c,i,c'])
     double* U = B.wd((size_t)r0 * n * r1);
-    B.gemm({gd(r0, n * r1, r0, Ln, 1, r0, X->core(0, k), 1, xc, U, 1, r0)});
+    GEMM(B, {gd(r0, n * r1, r0, Ln, 1, r0, xcore(k), 1, xc, U, 1, r0)});
     GemmDesc q{};
     q.m = r1; q.n = r1; q.k = r0 * n; q.batch = 1;
     q.m0 = r1; q.n0 = r1; q.k0e = r0;
-    q.A = X->core(0, k); q.a_i0 = (long long)xc * n; q.a_i1 = 0; q.a_k0 = 1; q.a_k1 = xc;
+    q.A = xcore(k); q.a_i0 = (long long)xc * n; q.a_i1 = 0; q.a_k0 = 1; q.a_k1 = xc;
     q.B = U; q.b_k0 = 1; q.b_k1 = r0; q.b_j0 = (long long)r0 * n; q.b_j1 = 0;
     q.C = Ln1; q.c_i0 = 1; q.c_i1 = 0; q.c_j0 = r1; q.c_j1 = 0;
     q.alpha = 1.0; q.beta = 0.0;
-    B.gemm({q});
+    GEMM(B, {q});
   };
   run_once(c, [&](Builder& B) {
-    B.copy({cd2(B.ctx->d_one, Lh_ck[0], 1, 1, 0, 0, 0, 0), cd2(B.ctx->d_one, Ln_ck[0], 1, 1, 0, 0, 0, 0)});
+    set_one(B, Lh_ck[0]);
+    set_one(B, Ln_ck[0]);
     double* curH = Lh_ck[0];
     double* curN = Ln_ck[0];
     for (int k = 0; k < N; ++k) {
@@ -670,7 +843,14 @@ void rayleigh_grad_host(ttc_context* c, const ttc_tto* Hh, const ttc_ttv* x, int
       emit_left_step(B, k, curH, curN, nh, nn);
       curH = nh; curN = nn;
     }
-    B.copy({cd2(curH, dval, 1, 1, 0, 0, 0, 0), cd2(curN, dval + 1, 1, 1, 0, 0, 0, 0)});
+    if (f32) {
+      CvtDesc w1{}, w2{};
+      w1.src = curH; w1.dst = dval; w1.rows = 1; w1.cols = 1; w1.ss_i = 1; w1.ds_i = 1; w1.alpha = 1.0;
+      w2 = w1; w2.src = curN; w2.dst = dval + 1;
+      B.widen({w1, w2});
+    } else {
+      B.copy({cd2(curH, dval, 1, 1, 0, 0, 0, 0), cd2(curN, dval + 1, 1, 1, 0, 0, 0, 0)});
+    }
   });
   double hv[2];
   TTC_CUDA(cudaMemcpy(hv, dval, sizeof(hv), cudaMemcpyDeviceToHost));
@@ -681,7 +861,8 @@ void rayleigh_grad_host(ttc_context* c, const ttc_tto* Hh, const ttc_ttv* x, int
   // pass 2: right-to-left, recomputing each segment's left environments from its checkpoint
   run_once(c, [&](Builder& B) {
     double* Rh = B.wd(1); double* Rn = B.wd(1);
-    B.copy({cd2(B.ctx->d_one, Rh, 1, 1, 0, 0, 0, 0), cd2(B.ctx->d_one, Rn, 1, 1, 0, 0, 0, 0)});
+    set_one(B, Rh);
+    set_one(B, Rn);
     int seg_lo = -1;
     std::vector<double*> segH(N + 1, nullptr), segN(N + 1, nullptr);
     for (int k = N - 1; k >= 0; --k) {
@@ -699,55 +880,61 @@ void rayleigh_grad_host(ttc_context* c, const ttc_tto* Hh, const ttc_ttv* x, int
       const int xc = X->capr(0, k);
       const double* Lh = segH[k];
       const double* Ln = segN[k];
-      double* G = dG + goff[k];
+      double* G = gcore(k);
       // Heff x: U[(c, j), (d, e)] = sum_f x[c,j,f] R[d,e,f]
       double* U = B.wd((size_t)r0 * n * r1 * R1);
       // right environments are stored (ket f, H e, bra d): R[f + r1*e + r1*R1*d]
-      GemmDesc u = gd(r0 * n, r1 * R1, r1, X->core(0, k), 1, (long long)xc * n, Rh, 1, (long long)r1 * R1, U, 1, (long long)r0 * n);
+      GemmDesc u = gd(r0 * n, r1 * R1, r1, xcore(k), 1, (long long)xc * n, Rh, 1, (long long)r1 * R1, U, 1, (long long)r0 * n);
       u.m0 = r0; u.a_i0 = 1; u.a_i1 = xc; u.c_i0 = 1; u.c_i1 = r0;
       u.n0 = r1; u.b_j0 = (long long)r1 * R1; u.b_j1 = r1;
       u.c_j0 = (long long)r0 * n; u.c_j1 = (long long)r0 * n * r1;   // U layout (c, j, d, e)
-      B.gemm({u});
+      GEMM(B, {u});
       // V[(b, c), (i, d)] = sum_{(j, e)} U[c, j, d, e] H[b, i, j, e]   (U layout (c, j, d, e))
       double* V = B.wd((size_t)R0 * r0 * n * r1);
       GemmDesc w{};
       w.m = r0 * r1; w.n = R0 * n; w.k = n * R1; w.batch = 1;
       w.m0 = r0; w.n0 = R0; w.k0e = n;
       w.A = U; w.a_i0 = 1; w.a_i1 = (long long)r0 * n; w.a_k0 = r0; w.a_k1 = (long long)r0 * n * r1;
-      w.B = H->core(k); w.b_k0 = (long long)R0 * n; w.b_k1 = (long long)R0 * n * n; w.b_j0 = 1; w.b_j1 = R0;
+      w.B = hcore(k); w.b_k0 = (long long)R0 * n; w.b_k1 = (long long)R0 * n * n; w.b_j0 = 1; w.b_j1 = R0;
       // V layout (b, c, i, d): b -> 1, c -> R0, i -> R0*r0, d -> R0*r0*n
       w.C = V; w.c_i0 = R0; w.c_i1 = (long long)R0 * r0 * n; w.c_j0 = 1; w.c_j1 = (long long)R0 * r0;
       w.alpha = 1.0; w.beta = 0.0;
-      B.gemm({w});
+      GEMM(B, {w});
       // G[a, (i, d)] = (2/nn) sum_{(b, c)} L[a, b, c] V[(b, c), (i, d)]
-      B.gemm({gd(r0, n * r1, R0 * r0, Lh, 1, r0, V, 1, (long long)R0 * r0, G, 1, r0, 2.0 / nn)});
+      GEMM(B, {gd(r0, n * r1, R0 * r0, Lh, 1, r0, V, 1, (long long)R0 * r0, G, 1, r0, 2.0 / nn)});
       // Neff x: T[(c, i), d] = sum_f x[c,i,f] Rn[d,f]; G -= (2R/nn) Ln[a,c] T[c,(i,d)]
       double* T = B.wd((size_t)r0 * n * r1);
-      GemmDesc t = gd(r0 * n, r1, r1, X->core(0, k), 1, (long long)xc * n, Rn, r1, 1, T, 1, (long long)r0 * n);
+      GemmDesc t = gd(r0 * n, r1, r1, xcore(k), 1, (long long)xc * n, Rn, r1, 1, T, 1, (long long)r0 * n);
       t.m0 = r0; t.a_i0 = 1; t.a_i1 = xc; t.c_i0 = 1; t.c_i1 = r0;
-      B.gemm({t});
-      B.gemm({gd(r0, n * r1, r0, Ln, 1, r0, T, 1, r0, G, 1, r0, -2.0 * Rq / nn, 1.0)});
+      GEMM(B, {t});
+      GEMM(B, {gd(r0, n * r1, r0, Ln, 1, r0, T, 1, r0, G, 1, r0, -2.0 * Rq / nn, 1.0)});
       // right environments at k: R_k[d0, e0, f0] = sum x[d0,i,d] H[e0,i,j,e] x[f0,j,f] R[d,e,f]
       double* Rh_new = B.wd((size_t)r0 * R0 * r0);
       double* Rn_new = B.wd((size_t)r0 * r0);
       OpEnvStep st{};
-      st.A = X->core(0, k); st.r = r0; st.xc = xc; st.r1 = r1;
-      st.H = H->core(k); st.R = R0; st.R1 = R1; st.n = n;
+      st.A = xcore(k); st.r = r0; st.xc = xc; st.r1 = r1;
+      st.H = hcore(k); st.R = R0; st.R1 = R1; st.n = n;
       st.g = r1; st.cdim = r0;
-      st.S = X->core(0, k); st.s_k = xc; st.s_c = 1;
+      st.S = xcore(k); st.s_k = xc; st.s_c = 1;
       st.V = Rh; st.W = Rh_new; st.batch = 1; st.v_b = st.s_b = st.w_b = 0;
       // stored (ket, H, bra), the layout the U contraction above reads
-      emit_op_env(B, {st});
+      emit_op_env(B, {st}, f32);
       double* Tn = B.wd((size_t)r0 * n * r1);
-      GemmDesc a1 = gd(r0 * n, r1, r1, X->core(0, k), 1, (long long)xc * n, Rn, 1, r1, Tn, 1, (long long)r0 * n);
+      GemmDesc a1 = gd(r0 * n, r1, r1, xcore(k), 1, (long long)xc * n, Rn, 1, r1, Tn, 1, (long long)r0 * n);
       a1.m0 = r0; a1.a_i0 = 1; a1.a_i1 = xc; a1.c_i0 = 1; a1.c_i1 = r0;
-      B.gemm({a1});
-      B.gemm({gd(r0, r0, n * r1, Tn, 1, r0, X->core(0, k), xc, 1, Rn_new, 1, r0)});
+      GEMM(B, {a1});
+      GEMM(B, {gd(r0, r0, n * r1, Tn, 1, r0, xcore(k), xc, 1, Rn_new, 1, r0)});
       Rh = Rh_new; Rn = Rn_new;
     }
   });
   std::vector<double> hg(gsz);
-  TTC_CUDA(cudaMemcpy(hg.data(), dG, gsz * sizeof(double), cudaMemcpyDeviceToHost));
+  if (f32) {
+    std::vector<float> hf(gsz);
+    TTC_CUDA(cudaMemcpy(hf.data(), dG, gsz * sizeof(float), cudaMemcpyDeviceToHost));
+    for (size_t e = 0; e < gsz; ++e) hg[e] = hf[e];
+  } else {
+    TTC_CUDA(cudaMemcpy(hg.data(), dG, gsz * sizeof(double), cudaMemcpyDeviceToHost));
+  }
   // internal (a, i, d) -> Julia (i, a, d)
   for (int k = 0; k < N; ++k) {
     const int r0 = rk(k), r1 = rk(k + 1), n = (int)X->dims[k];

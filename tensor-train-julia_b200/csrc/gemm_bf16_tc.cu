@@ -231,11 +231,14 @@ __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc*
           const int col = col0 + c0 + i;
           if (col < D.n) {
             const double x = D.alpha * (double)v[i];
-            if (D.C64) D.C64[roff64 + (long long)col * D.c_j] = x;
-            if (D.C32) reinterpret_cast<float*>(D.C32)[roff64 + (long long)col * D.c_j] = (float)x;
+            const int j1 = D.n0 > 0 ? col / D.n0 : 0, j0 = col - j1 * D.n0;
+            const long long co64 = (long long)j0 * D.c_j + (long long)j1 * D.c_j1;
+            if (D.C64) D.C64[roff64 + co64] = x;
+            if (D.C32) reinterpret_cast<float*>(D.C32)[roff64 + co64] = (float)x;
             if (D.C16) {   // operand-typed output
-              if constexpr (TF32) reinterpret_cast<float*>(D.C16)[roff16 + (long long)col * D.h_j] = round_tf32((float)x);
-              else reinterpret_cast<__nv_bfloat16*>(D.C16)[roff16 + (long long)col * D.h_j] = __double2bfloat16(x);
+              const long long co16 = (long long)j0 * D.h_j + (long long)j1 * D.h_j1;
+              if constexpr (TF32) reinterpret_cast<float*>(D.C16)[roff16 + co16] = round_tf32((float)x);
+              else reinterpret_cast<__nv_bfloat16*>(D.C16)[roff16 + co16] = __double2bfloat16(x);
             }
           }
         }

@@ -71,6 +71,8 @@ void rand_rounding_host(ttc_context* c, int m, const double* alpha, const ttc_tt
 // W[k] / sqrt(p_k) as (r_k, s_k) (TT) or (r_k, R_k, s_k) (operator) column-major.
 void emit_sketch_op_f64(Builder& B, const DevTTO& H, ttc_batch* x, int t, const SketchPlan& sp,
                         const std::vector<double*>& S, std::vector<double*>& W);
+void emit_sketch_op_tc(Builder& B, const DevTTO& H, ttc_batch* x, int t, const SketchPlan& sp,
+                       const std::vector<double*>& S, std::vector<double*>& W, bool tf32);
 
 void recursive_sketch_host(ttc_context* c, const ttc_ttv* Ah, const ttc_tto* Hh, const int64_t* rks,
                            const ttc_sketch_opts& sk, double* const* W_out, int64_t* sketch_rks) {
@@ -112,7 +114,8 @@ void recursive_sketch_host(ttc_context* c, const ttc_ttv* Ah, const ttc_tto* Hh,
     emit_sketch_blocks(B, xb->dims, sp, sk, raw, S);
     std::vector<double*> Wk;
     if (H) {
-      emit_sketch_op_f64(B, *H, xb, 0, sp, S, Wk);
+      if (tensor_core_sketch(sk.precision)) emit_sketch_op_tc(B, *H, xb, 0, sp, S, Wk, sk.precision == TTC_PREC_TF32);
+      else emit_sketch_op_f64(B, *H, xb, 0, sp, S, Wk);
     } else {
       std::vector<std::vector<double*>> W;
       if (tensor_core_sketch(sk.precision)) emit_sketch_bf16(B, xb, {0}, sp, S, W, sk.precision == TTC_PREC_TF32);

@@ -6,6 +6,8 @@ namespace ttc {
 
 // ---- grouped FP64 GEMM (gemm_f64.cu)
 void launch_gemm_f64(const GemmDesc* d_descs, int nd, long long total_tiles, cudaStream_t s);
+// ---- the same problems with float data in A, B and C, FP32 accumulation (gemm_f32.cu)
+void launch_gemm_f32(const GemmDesc* d_descs, int nd, long long total_tiles, cudaStream_t s);
 long long gemm_tiles(const GemmDesc& d);
 
 // Device-side size bound: min(cap, mult * *p) when p is given (a rank that an earlier kernel of
@@ -129,11 +131,13 @@ struct Bf16GemmDesc {
   int m, n, k, m0;                // m0: row split (row i = i0 + m0*i1) of the outputs
   const void* A; long long lda;   // operand type, K-major: A(i, kk) at A[i*lda + kk]
   const void* B; long long ldb;   // operand type, K-major: B(j, kk) at B[j*ldb + kk]
-  double* C64; float* C32;        // outputs sharing strides: (i0*c_i0 + i1*c_i1 + j*c_j)
-  void* C16;                      // output in the operand type (BF16 or FP32), strides (h_i0, h_i1, h_j)
+  double* C64; float* C32;        // outputs sharing strides: (i0*c_i0 + i1*c_i1 + j0*c_j + j1*c_j1)
+  void* C16;                      // output in the operand type (BF16 or FP32), strides (h_i0, h_i1, h_j, h_j1)
   long long c_i0, c_i1, c_j, h_i0, h_i1, h_j;
   double alpha;
   long long tile_start;
+  int n0;                         // column split j = j0 + n0*j1 of the outputs (0: no split)
+  long long c_j1, h_j1;
 };
 void launch_gemm_bf16_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags,
                          bool tf32 = false);

@@ -46,6 +46,38 @@ void launch_setrank(const SetRankDesc* d, int count, cudaStream_t s) {
   TTC_CHECK_LAUNCH();
 }
 
+__global__ void cvt_f32_kernel(const CvtDesc* descs) {
+  const CvtDesc D = descs[blockIdx.y];
+  const long long total = D.rows * D.cols;
+  float* dst = reinterpret_cast<float*>(D.dst);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e % D.rows, j = e / D.rows;
+    dst[i * D.ds_i + j * D.ds_j] = (float)(D.alpha * D.src[i * D.ss_i + j * D.ss_j]);
+  }
+}
+void launch_cvt_f32(const CvtDesc* d, int count, long long max_elems, cudaStream_t s) {
+  if (count <= 0 || max_elems <= 0) return;
+  const long long blocks = std::min<long long>((max_elems + 255) / 256, 148LL * 8);
+  cvt_f32_kernel<<<dim3((unsigned)blocks, (unsigned)count), 256, 0, s>>>(d);
+  TTC_CHECK_LAUNCH();
+}
+__global__ void widen_kernel(const CvtDesc* descs) {
+  const CvtDesc D = descs[blockIdx.y];
+  const long long total = D.rows * D.cols;
+  const float* src = reinterpret_cast<const float*>(D.src);
+  double* dst = reinterpret_cast<double*>(D.dst);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e % D.rows, j = e / D.rows;
+    dst[i * D.ds_i + j * D.ds_j] = D.alpha * (double)src[i * D.ss_i + j * D.ss_j];
+  }
+}
+void launch_widen(const CvtDesc* d, int count, long long max_elems, cudaStream_t s) {
+  if (count <= 0 || max_elems <= 0) return;
+  const long long blocks = std::min<long long>((max_elems + 255) / 256, 148LL * 8);
+  widen_kernel<<<dim3((unsigned)blocks, (unsigned)count), 256, 0, s>>>(d);
+  TTC_CHECK_LAUNCH();
+}
+
 template <typename T>
 __global__ void cvt_bf16_kernel(const CvtDesc* descs) {
   const CvtDesc D = descs[blockIdx.y];
@@ -98,6 +130,9 @@ static void launch_op(ttc_context* c, const Plan& p, const Op& op) {
       case OP_ZERO: launch_zero((const ZeroDesc*)d, op.count, op.total, s); break;
       case OP_SUMSQ: launch_sumsq((const NormDesc*)d, op.count, s); break;
       case OP_APPLY: launch_apply((const ApplyDesc*)d, op.count, op.total, s); break;
+      case OP_GEMM32: launch_gemm_f32((const GemmDesc*)d, op.count, op.total, s); break;
+      case OP_CVT32: launch_cvt_f32((const CvtDesc*)d, op.count, op.total, s); break;
+      case OP_WIDEN: launch_widen((const CvtDesc*)d, op.count, op.total, s); break;
       case OP_PHILOX: launch_philox((const PhiloxDesc*)d, op.count, op.total, s); break;
       case OP_BF16GEMM: launch_gemm_bf16_tc((const Bf16GemmDesc*)d, op.count, op.total, s, c->d_flags, op.a != 0); break;
       case OP_ZEROCHK: launch_zerochk((const ZeroChkDesc*)d, op.count, s); break;
@@ -118,6 +153,7 @@ long long count_launches(const Plan& p) {
 static int op_kind(OpKind k) {
   switch (k) {
     case OP_GEMM: return TTC_KERN_GEMM_F64;
+    case OP_GEMM32: return TTC_KERN_GEMM_F64;
     case OP_QR: return TTC_KERN_QR;
     case OP_QAPPLY: return TTC_KERN_QR;
     case OP_JACOBI: return TTC_KERN_JACOBI;
@@ -303,18 +339,18 @@ inline long long sp2(long long e0, long long s0, long long e1, long long s1) {
   const long long e[2] = {e0, e1}, s[2] = {s0, s1};
   return span_elems(e, s, 2);
 }
-void check_gemm(const GemmDesc& d) {
+void check_gemm(const GemmDesc& d, size_t esz = 8) {
   const long long mi0 = std::min(d.m, d.m0), mi1 = (d.m - 1) / d.m0 + 1;
   const long long ni0 = std::min(d.n, d.n0), ni1 = (d.n - 1) / d.n0 + 1;
   const long long ki0 = std::min(d.k, d.k0e), ki1 = (d.k - 1) / d.k0e + 1;
   if (d.k > 0) {
     const long long ea[5] = {mi0, mi1, ki0, ki1, d.batch}, sa[5] = {d.a_i0, d.a_i1, d.a_k0, d.a_k1, d.a_b};
-    region_check(d.A, 8 * (size_t)span_elems(ea, sa, 5), "gemm A");
+    region_check(d.A, esz * (size_t)span_elems(ea, sa, 5), "gemm A");
     const long long eb[5] = {ki0, ki1, ni0, ni1, d.batch}, sb[5] = {d.b_k0, d.b_k1, d.b_j0, d.b_j1, d.b_b};
-    region_check(d.B, 8 * (size_t)span_elems(eb, sb, 5), "gemm B");
+    region_check(d.B, esz * (size_t)span_elems(eb, sb, 5), "gemm B");
   }
   const long long ec[5] = {mi0, mi1, ni0, ni1, d.batch}, sc[5] = {d.c_i0, d.c_i1, d.c_j0, d.c_j1, d.c_b};
-  region_check(d.C, 8 * (size_t)span_elems(ec, sc, 5), "gemm C");
+  region_check(d.C, esz * (size_t)span_elems(ec, sc, 5), "gemm C");
   if (d.n_dev) region_check(d.n_dev, sizeof(int), "gemm n_dev");
 }
 }  // namespace
@@ -361,6 +397,51 @@ void Builder::gemm(std::vector<GemmDesc> v) {
   if (w.empty()) return;
   Op op; op.kind = OP_GEMM; op.off = plan->push(w); op.count = (int)w.size(); op.total = t;
   for (auto& d : w) op.flops += 2.0 * d.m * d.n * d.k * std::max(1, d.batch);
+  plan->ops.push_back(op);
+}
+void Builder::gemm32(std::vector<GemmDesc> v) {
+  std::vector<GemmDesc> w;
+  long long t = 0;
+  for (auto& d : v) {
+    const long long n = gemm_tiles(d);
+    if (n == 0) continue;
+    if (d.m0 <= 0) d.m0 = std::max(d.m, 1);
+    if (d.n0 <= 0) d.n0 = std::max(d.n, 1);
+    if (d.k0e <= 0) d.k0e = std::max(d.k, 1);
+    if (wsbase) check_gemm(d, 4);
+    d.tile_start = t;
+    t += n;
+    w.push_back(d);
+  }
+  if (w.empty()) return;
+  Op op; op.kind = OP_GEMM32; op.off = plan->push(w); op.count = (int)w.size(); op.total = t;
+  for (auto& d : w) op.flops += 2.0 * d.m * d.n * d.k * std::max(1, d.batch);
+  plan->ops.push_back(op);
+}
+void Builder::cvt_f32(const std::vector<CvtDesc>& v) {
+  if (v.empty()) return;
+  long long mx = 0;
+  for (auto& d : v) {
+    mx = std::max(mx, d.rows * d.cols);
+    if (wsbase) {
+      region_check(d.src, 8 * (size_t)sp2(d.rows, d.ss_i, d.cols, d.ss_j), "cvt32 src");
+      region_check(d.dst, 4 * (size_t)sp2(d.rows, d.ds_i, d.cols, d.ds_j), "cvt32 dst");
+    }
+  }
+  Op op; op.kind = OP_CVT32; op.off = plan->push(v); op.count = (int)v.size(); op.total = mx;
+  plan->ops.push_back(op);
+}
+void Builder::widen(const std::vector<CvtDesc>& v) {
+  if (v.empty()) return;
+  long long mx = 0;
+  for (auto& d : v) {
+    mx = std::max(mx, d.rows * d.cols);
+    if (wsbase) {
+      region_check(d.src, 4 * (size_t)sp2(d.rows, d.ss_i, d.cols, d.ss_j), "widen src");
+      region_check(d.dst, 8 * (size_t)sp2(d.rows, d.ds_i, d.cols, d.ds_j), "widen dst");
+    }
+  }
+  Op op; op.kind = OP_WIDEN; op.off = plan->push(v); op.count = (int)v.size(); op.total = mx;
   plan->ops.push_back(op);
 }
 void Builder::qr(const std::vector<QRDesc>& v) {
@@ -516,14 +597,16 @@ void Builder::bf16gemm(std::vector<Bf16GemmDesc> v, bool tf32) {
       region_check(d.A, esz * (size_t)(d.lda * (d.m - 1) + kp), "bf16 A");
       region_check(d.B, esz * (size_t)(d.ldb * (d.n - 1) + kp), "bf16 B");
       const long long mi0 = std::min(d.m, d.m0), mi1 = (d.m - 1) / d.m0 + 1;
+      TTC_REQUIRE(d.n0 >= 0, TTC_EINTERNAL, "bf16 gemm: negative column split");
+      const long long nj0 = d.n0 > 0 ? std::min(d.n, d.n0) : d.n, nj1 = d.n0 > 0 ? (d.n - 1) / d.n0 + 1 : 1;
       if (d.C64 || d.C32) {
-        const long long e[3] = {mi0, mi1, d.n}, s[3] = {d.c_i0, d.c_i1, d.c_j};
-        if (d.C64) region_check(d.C64, 8 * (size_t)span_elems(e, s, 3), "bf16 C64");
-        if (d.C32) region_check(d.C32, 4 * (size_t)span_elems(e, s, 3), "bf16 C32");
+        const long long e[4] = {mi0, mi1, nj0, nj1}, s[4] = {d.c_i0, d.c_i1, d.c_j, d.c_j1};
+        if (d.C64) region_check(d.C64, 8 * (size_t)span_elems(e, s, 4), "bf16 C64");
+        if (d.C32) region_check(d.C32, 4 * (size_t)span_elems(e, s, 4), "bf16 C32");
       }
       if (d.C16) {
-        const long long e[3] = {mi0, mi1, d.n}, s[3] = {d.h_i0, d.h_i1, d.h_j};
-        region_check(d.C16, esz * (size_t)span_elems(e, s, 3), "bf16 C16");
+        const long long e[4] = {mi0, mi1, nj0, nj1}, s[4] = {d.h_i0, d.h_i1, d.h_j, d.h_j1};
+        region_check(d.C16, esz * (size_t)span_elems(e, s, 4), "bf16 C16");
       }
     }
     d.tile_start = t;

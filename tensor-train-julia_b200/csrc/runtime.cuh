@@ -22,7 +22,8 @@ constexpr int kEvRunBegin = 6, kEvRunEnd = 7;
 
 enum OpKind {
   OP_GEMM, OP_QR, OP_JACOBI, OP_TRUNC, OP_SELECT, OP_COPY, OP_ZERO, OP_SUMSQ, OP_APPLY,
-  OP_PHILOX, OP_BF16GEMM, OP_ZEROCHK, OP_FINAL, OP_STAGE, OP_CVT_BF16, OP_SETRANK, OP_QAPPLY
+  OP_PHILOX, OP_BF16GEMM, OP_ZEROCHK, OP_FINAL, OP_STAGE, OP_CVT_BF16, OP_SETRANK, OP_QAPPLY, OP_GEMM32, OP_CVT32,
+  OP_WIDEN
 };
 
 struct Op {
@@ -55,6 +56,11 @@ void launch_final(const FinalDesc* d, int count, long long max_n, cudaStream_t s
 void launch_setrank(const SetRankDesc* d, int count, cudaStream_t s);
 // FP64 -> BF16 (f32 = false) or FP64 -> FP32 rounded to TF32 (f32 = true), same index map.
 void launch_cvt_bf16(const CvtDesc* d, int count, long long max_elems, cudaStream_t s, bool f32 = false);
+// FP64 -> FP32 (round to nearest), same index map.
+void launch_cvt_f32(const CvtDesc* d, int count, long long max_elems, cudaStream_t s);
+// FP32 -> FP64: dst (double) from src holding floats, same index map (CvtDesc with the roles of the
+// pointers swapped: `src` points to floats, `dst` to doubles).
+void launch_widen(const CvtDesc* d, int count, long long max_elems, cudaStream_t s);
 
 struct Plan {
   std::vector<unsigned char> blob;

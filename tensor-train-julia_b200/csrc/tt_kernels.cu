@@ -192,22 +192,26 @@ void launch_select(const SelectDesc* d, int count, int max_rows, int max_cols, c
 // Y[(a + R*nu), i, (a' + R'*nu')] = sum_j H[a, i, j, a'] * V[nu, j, nu'] (internal layouts;
 // src/tt_operations.jl:184).  One thread per output element, consecutive threads on the
 // fastest output index a, so H is read coalesced and V is a broadcast.  HBM-bound on Y.
+// Output element e = u + U w with u = a + R nu (the combined left rank index, operator index
+// fastest) and w = i + n (an + R' nun): consecutive threads write consecutive elements, and each
+// reads its n operator entries and n vector entries (shared by the R threads of one nu and the r
+// threads of one a, so they come from L1).  The HBM traffic is the output's write stream.
+template <typename I>
 __global__ void apply_kernel(const ApplyDesc* __restrict__ descs) {
   const ApplyDesc D = descs[blockIdx.y];
-  const long long Rr = (long long)D.R * D.r, Rrn = (long long)D.Rn * D.rn;
-  const long long total = Rr * D.n * Rrn;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-    long long t = e;
-    const int a = (int)(t % D.R); t /= D.R;
-    const int nu = (int)(t % D.r); t /= D.r;
-    const int i = (int)(t % D.n); t /= D.n;
-    const int an = (int)(t % D.Rn); const int nun = (int)(t / D.Rn);
+  const I R = (I)D.R, n = (I)D.n, Rn = (I)D.Rn;
+  const I U = R * (I)D.r;
+  const I total = U * n * Rn * (I)D.rn;
+  const long long hj = (long long)D.R * D.n;          // H stride of j
+  for (I e = (I)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (I)gridDim.x * blockDim.x) {
+    const I u = e % U, w = e / U;
+    const I nu = u / R, a = u - nu * R;
+    const I i = w % n, t = w / n;
+    const I an = t % Rn, nun = t / Rn;
+    const double* h = D.H + a + (long long)R * i + hj * n * (long long)an;
+    const double* v = D.V + nu + (long long)D.r * n * (long long)nun;
     double acc = 0.0;
-    for (int j = 0; j < D.n; ++j) {
-      const double h = D.H[a + (long long)D.R * (i + (long long)D.n * (j + (long long)D.n * an))];
-      const double v = D.V[nu + (long long)D.r * (j + (long long)D.n * nun)];
-      acc = fma(h, v, acc);
-    }
+    for (int j = 0; j < D.n; ++j) acc = fma(h[hj * j], v[(long long)D.r * j], acc);
     D.Y[e] = acc;
   }
 }
@@ -215,7 +219,8 @@ __global__ void apply_kernel(const ApplyDesc* __restrict__ descs) {
 void launch_apply(const ApplyDesc* d, int count, long long max_elems, cudaStream_t s) {
   if (count <= 0 || max_elems <= 0) return;
   const long long blocks = std::min<long long>((max_elems + NT - 1) / NT, 148LL * 16);
-  apply_kernel<<<dim3((unsigned)blocks, (unsigned)count), NT, 0, s>>>(d);
+  if (max_elems < (1LL << 31)) apply_kernel<unsigned><<<dim3((unsigned)blocks, (unsigned)count), NT, 0, s>>>(d);
+  else apply_kernel<unsigned long long><<<dim3((unsigned)blocks, (unsigned)count), NT, 0, s>>>(d);
   TTC_CHECK_LAUNCH();
 }
 

@@ -549,14 +549,19 @@ def tt_scale(a: float, x: TTvector) -> TTvector:
     return out.tt()
 
 
-def rayleigh_grad(H: TToperator, x: TTvector, ckpt_every: int = 4):
-    """Value and gradient of <x|H|x>/<x|x> with respect to every core of x (H symmetric)."""
+def rayleigh_grad(H: TToperator, x: TTvector, ckpt_every: int = 4, precision: str = "fp64"):
+    """Value and gradient of <x|H|x>/<x|x> with respect to every core of x (H symmetric), with
+    the contractions in FP64 or in FP32 with FP32 accumulation (precision="fp32")."""
+    prec = {"fp64": 0, "fp32": 3}.get(precision)
+    if prec is None:
+        raise ArgumentError(f"precision must be 'fp64' or 'fp32', not {precision!r}")
     ctx = get_context()
     keep = _Keep()
     hs, xs = _tto(H, keep), _ttv(x, keep)
     G = [np.empty(c.size, dtype=np.float64) for c in x.ttv_vec]
     v = C.c_double()
-    ctx.check(lib.ttc_rayleigh_grad(ctx.h, C.byref(hs), C.byref(xs), int(ckpt_every), C.byref(v), _ptrs(G, keep)))
+    ctx.check(lib.ttc_rayleigh_grad_prec(ctx.h, C.byref(hs), C.byref(xs), int(ckpt_every), prec, C.byref(v),
+                                         _ptrs(G, keep)))
     return v.value, [G[k].reshape(x.ttv_vec[k].shape, order="F") for k in range(x.N)]
 
 

@@ -94,6 +94,7 @@ _SIGS = {
     "ttc_tt_add": (i32, [vp, C.POINTER(TTV), C.POINTER(TTV), C.POINTER(TTVOut)]),
     "ttc_tt_scale": (i32, [vp, f64, C.POINTER(TTV), C.POINTER(TTVOut)]),
     "ttc_rayleigh_grad": (i32, [vp, C.POINTER(TTO), C.POINTER(TTV), i32, P_f64, PP_f64]),
+    "ttc_rayleigh_grad_prec": (i32, [vp, C.POINTER(TTO), C.POINTER(TTV), i32, i32, P_f64, PP_f64]),
     "ttc_qr_noalloc": (i32, [i32, i32, vp, i64, vp, i64, vp, i64, vp, vp]),
     "ttc_host_alloc": (i32, [sz, C.POINTER(vp)]),
     "ttc_host_free": (i32, [vp]),
