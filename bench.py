@@ -227,13 +227,14 @@ def rand_cores(dims, ranks, g, normalise=False):
     return out
 
 
-def device_ms(ctx, fn, reps):
-    """Device time of `reps` calls of fn (events on the library's stream), after one warm-up call."""
+def device_ms(ctx, fn, reps, stream):
+    """Device time of `reps` calls of fn (events on `stream`, the library's stream), after one
+    warm-up call."""
     import torch
     fn()
     ctx.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    st = torch.cuda.current_stream()
+    st = stream
     e0.record(st)
     for _ in range(reps):
         fn()
@@ -243,7 +244,7 @@ def device_ms(ctx, fn, reps):
     return e0.elapsed_time(e1) / reps
 
 
-def other_configs(ttcuda, ctx, hbm_peak):
+def other_configs(ttcuda, ctx, hbm_peak, stream):
     """Configs 1, 2 and 4 of the benchmark set, each through the library's public API on host
     tensors (end to end, transfers included) and, where one kernel bounds it, with that kernel's
     device time from the per-kernel profile."""
@@ -257,10 +258,10 @@ def other_configs(ttcuda, ctx, hbm_peak):
     for j in range(1, 9):
         t = ttcuda.tt_scale(2.0 ** -j, ttcuda.TTvector(20, rand_cores(dims, r8, g), dims, r8))
         X = t if X is None else ttcuda.tt_add(X, t)
-    ms1 = device_ms(ctx, lambda: ttcuda.tt_rounding(X, tol=1e-8, rmax=64), 20)
+    ms1 = device_ms(ctx, lambda: ttcuda.tt_rounding(X, tol=1e-8, rmax=64), 20, stream)
     xb = ttcuda.DeviceBatch.from_tts([X], ctx=ctx)
     yb = ttcuda.DeviceBatch(dims, [X.ttv_rks], ctx=ctx)
-    ms1d = device_ms(ctx, lambda: xb.round_det(yb, tol=1e-8, rmax=64, sync=False), 50)
+    ms1d = device_ms(ctx, lambda: xb.round_det(yb, tol=1e-8, rmax=64, sync=False), 50, stream)
     Y = yb.download()[0]
     out["config1"] = {"workload": "tt_rounding(X; tol=1e-8, rmax=64), X = sum of 8 rank-8 N(0,1) TTs scaled 2^-j, "
                                   "n=2, d=20 (input ranks up to 64)",
@@ -278,20 +279,25 @@ def other_configs(ttcuda, ctx, hbm_peak):
     Hy = ttcuda.mpo_apply(H, y)
     prof = ctx.kernel_profile()["mpo_apply"]
     ctx.set_profiling(False)
-    ms_apply = device_ms(ctx, lambda: ttcuda.mpo_apply(H, y), 5)
+    ms_apply = device_ms(ctx, lambda: ttcuda.mpo_apply(H, y), 5, stream)
     out_bytes = sum(8 * 2 * Hy.ttv_rks[k] * Hy.ttv_rks[k + 1] for k in range(32))
     in_bytes = sum(8 * c.size for c in y.ttv_vec) + sum(8 * c.size for c in H.tto_vec)
     kern_ms = prof[0] / max(1, prof[1]) * prof[1]      # device time of all apply launches of one call
     gbs = (out_bytes + in_bytes) / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else None
     rks = [1] + [138] * 31 + [1]
     ms_op = device_ms(ctx, lambda: ttcuda.ttrand_rounding_op([1.0], H, [y], rks, orthogonal=False, seed=5,
-                                                             block_rks=138), 3)
+                                                             block_rks=138), 3, stream)
     ms_op_tf = device_ms(ctx, lambda: ttcuda.ttrand_rounding_op([1.0], H, [y], rks, orthogonal=False, seed=5,
-                                                                block_rks=138, precision="tf32"), 3)
+                                                                block_rks=138, precision="tf32"), 3, stream)
     z64 = ttcuda.ttrand_rounding_op([1.0], H, [y], rks, orthogonal=False, seed=5, block_rks=138)
     ztf = ttcuda.ttrand_rounding_op([1.0], H, [y], rks, orthogonal=False, seed=5, block_rks=138, precision="tf32")
     dz = ttcuda.tt_add(z64, ttcuda.tt_scale(-1.0, ztf))
     rel_tf = ttcuda.norm(dz) / ttcuda.norm(z64)
+
+    def err_vs_Hy(z):     # ||H y - z|| / ||H y|| from inner products (the error is far above their cancellation)
+        hh = ttcuda.dot(Hy, Hy)
+        return math.sqrt(max(0.0, hh - 2.0 * ttcuda.dot(Hy, z) + ttcuda.dot(z, z)) / hh)
+    err64, errtf = err_vs_Hy(z64), err_vs_Hy(ztf)
     out["config2"] = {"workload": "1D Hubbard MPO (hV_to_mpo on the GPU, 16 sites, t=1, U=4, MPO ranks up to "
                                   f"{max(H.tto_rks)}) x rank-128 N(0,1) TT; sketch rank 138 (block_rks=138)",
                       "apply": {"value": 1e3 / ms_apply, "unit": "contractions/s", "ms": ms_apply,
@@ -308,6 +314,7 @@ def other_configs(ttcuda, ctx, hbm_peak):
                                                  "path": "the same with the operator sketch on the tcgen05 tensor "
                                                          "cores (TF32 operands, FP32 accumulation), FP64 range finder",
                                                  "rel_diff_vs_fp64": rel_tf,
+                                                 "rel_err_vs_Hy": errtf, "rel_err_vs_Hy_fp64": err64,
                                                  "ranks_identical_fp64": ztf.ttv_rks == z64.ttv_rks}}
     # config 4: gradient of <x|H|x>/<x|x>, 4x4 open Hubbard (U=8) in snake ordering, x rank 256
     h4, V4 = tm.hubbard_2D(4, 4, t=1.0, U=8.0, w_pbc=False, L_pbc=False)
@@ -319,8 +326,8 @@ def other_configs(ttcuda, ctx, hbm_peak):
     ttcuda.rayleigh_grad(H4, x4, ckpt_every=4)
     prof4 = ctx.kernel_profile()["gemm_f64"]
     ctx.set_profiling(False)
-    ms_g = device_ms(ctx, lambda: ttcuda.rayleigh_grad(H4, x4, ckpt_every=4), 3)
-    ms_g32 = device_ms(ctx, lambda: ttcuda.rayleigh_grad(H4, x4, ckpt_every=4, precision="fp32"), 3)
+    ms_g = device_ms(ctx, lambda: ttcuda.rayleigh_grad(H4, x4, ckpt_every=4), 3, stream)
+    ms_g32 = device_ms(ctx, lambda: ttcuda.rayleigh_grad(H4, x4, ckpt_every=4, precision="fp32"), 3, stream)
     R64, G64 = ttcuda.rayleigh_grad(H4, x4, ckpt_every=4)
     R32, G32 = ttcuda.rayleigh_grad(H4, x4, ckpt_every=4, precision="fp32")
     gd = math.sqrt(sum(float(np.sum((a - b) ** 2)) for a, b in zip(G32, G64)))
@@ -335,6 +342,44 @@ def other_configs(ttcuda, ctx, hbm_peak):
                       "fp32": {"value": 1e3 / ms_g32, "unit": "gradients/s", "ms": ms_g32,
                                "variant": "FP32 cores and environments, FP32 accumulation",
                                "rel_diff_gradient_vs_fp64": gd / gn, "rel_diff_value_vs_fp64": abs(R32 - R64) / abs(R64)}}
+    # config 5 shapes: 48 sites, x of rank 512, operator-aware rounding to a rank-522 sketch (block_rks =
+    # 522) with the sketch contractions in BF16 on the tensor cores, FP32 accumulation, FP64 range
+    # finder and QR.  The 48-spin-orbital molecular MPO has rank ~2L^2+3L+2 = 1226 (L = 24 spatial
+    # orbitals); its roundings need Householder QRs of ~4900 rows, beyond the QR kernel's 1536, so a
+    # stand-in MPO of the same sites with ranks min(4^k, 4^(d-k), 192) and N(0,1)/sqrt(4 R_k) cores
+    # takes its place here.
+    d5, R5, r5, s5 = 48, 192, 512, 522
+    g5 = np.random.default_rng(55)
+    Rk = [min(4 ** min(k, d5 - k), R5) for k in range(d5 + 1)]
+    H5 = ttcuda.TToperator(d5, [np.asfortranarray(g5.standard_normal((2, 2, Rk[k], Rk[k + 1])) / math.sqrt(4 * Rk[k + 1]))
+                                for k in range(d5)], (2,) * d5, Rk)
+    dims5 = (2,) * d5
+    rx = r_and_d([1] + [r5] * (d5 - 1) + [1], dims5, r5)
+    x5 = ttcuda.TTvector(d5, rand_cores(dims5, rx, g5, normalise=True), dims5, rx)
+    rks5 = [1] + [s5] * (d5 - 1) + [1]
+    run5 = lambda prec: ttcuda.ttrand_rounding_op([1.0], H5, [x5], rks5, orthogonal=False, seed=5, block_rks=s5,  # noqa: E731
+                                                  precision=prec)
+    ms5b = device_ms(ctx, lambda: run5("bf16"), 2, stream)
+    ms5d = device_ms(ctx, lambda: run5("fp64"), 1, stream)
+    z5b, z5d = run5("bf16"), run5("fp64")
+    rel5 = ttcuda.norm(ttcuda.tt_add(z5d, ttcuda.tt_scale(-1.0, z5b))) / ttcuda.norm(z5d)
+    ctx.set_profiling(True)
+    run5("bf16")
+    prof5 = ctx.kernel_profile()
+    ctx.set_profiling(False)
+    tc = prof5["gemm_bf16_tcgen05"]
+    out["config5_shapes"] = {
+        "workload": f"operator-aware ttrand_rounding([1.0], H, [x], rks): d=48, n=2, x rank {r5} (N(0,1), "
+                    f"normalised), sketch rank {s5} (block_rks = {s5}, Gaussian), H a stand-in MPO of ranks "
+                    f"min(4^k, 4^(d-k), {R5}) (the 48-spin-orbital molecular MPO, rank ~1226, exceeds the QR "
+                    "kernel's 1536-row limit in its own rounding)",
+        "value": 1e3 / ms5b, "unit": "roundings/s", "ms": ms5b,
+        "variant": "BF16 operator sketch (tcgen05), FP32 accumulation; FP64 range finder, QR and projections",
+        "fp64": {"value": 1e3 / ms5d, "unit": "roundings/s", "ms": ms5d},
+        "rel_diff_vs_fp64": rel5, "ranks_identical_fp64": z5b.ttv_rks == z5d.ttv_rks,
+        "tcgen05_sketch": {"ms": tc[0], "launches": tc[1], "tflop": tc[2] / 1e12,
+                           "tflops": (tc[2] / (tc[0] / 1e3) / 1e12) if tc[0] > 0 else None},
+        "profile_ms": {k: round(v[0], 3) for k, v in prof5.items() if v[1]}}
     return out
 
 
@@ -516,7 +561,7 @@ def main():
             hbm_src = "MEASURED_PEAKS.json hbm_gbs (measured)"
         except Exception:
             pass
-        others = other_configs(ttcuda, ctx, hbm)
+        others = other_configs(ttcuda, ctx, hbm, stream)
         others["config2"]["apply"]["roofline"]["peak_source"] = hbm_src
 
     # end-to-end through the C ABI with host buffers (upload, round, download) every step; device

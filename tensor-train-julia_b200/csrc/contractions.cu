@@ -163,6 +163,12 @@ void emit_sketch_op_f64(Builder& B, const DevTTO& H, ttc_batch* x, int t, const 
 // G3 also W in FP64 (for the FP64 range finder) and the next site's V operand.  Operands are
 // zero-padded to 16-byte rows; the TT core, the MPO core and the sketch blocks are converted
 // once per call.
+// Precision policy (as for the TT sketch): the range finder stays exact under a perturbed sketch
+// only where the right interface of H y has full row rank.  Where it is structurally rank
+// deficient -- rho_k = min(r_k R_k, n_k rho_{k+1}) < r_k R_k, the bonds near the end whose
+// combined rank exceeds the dimension of the right part -- W_k must keep the form R_k X, which
+// rounding the operands breaks, so those levels are contracted in FP64 (from the FP64 W_{k+1})
+// and only their result is converted for the next tensor-core level.
 static inline long long pad_k(long long v, bool tf32) { const long long c = tf32 ? 4 : 8; return (v + c - 1) / c * c; }
 
 void emit_sketch_op_tc(Builder& B, const DevTTO& H, ttc_batch* x, int t, const SketchPlan& sp,
@@ -181,12 +187,22 @@ void emit_sketch_op_tc(Builder& B, const DevTTO& H, ttc_batch* x, int t, const S
   std::vector<void*> A16(N), H16(N), S16(N), V16(N + 1);
   std::vector<long long> ldv(N + 1);
   std::vector<CvtDesc> cv;
+  std::vector<char> f64lvl(N + 1, 0);
+  {
+    long long rho = 1;
+    for (int k = N - 1; k >= 0; --k) {
+      const long long full = (long long)x->rk(t, k) * H.rks[k];
+      rho = std::min<long long>(full, x->dims[k] * rho);
+      f64lvl[k] = rho < full;
+    }
+  }
   for (int k = 0; k < N; ++k) {
     const long long n = x->dims[k], r = x->rk(t, k), r1 = x->rk(t, k + 1), xc = x->capr(t, k);
     const long long R = H.rks[k], R1 = H.rks[k + 1], g = sp.b[k + 1], cd = sp.b[k], pk = sp.p[k];
     W[k] = B.wd((size_t)(r * R * cd * pk));
     ldv[k] = pad_k(r, tf32);
     V16[k] = (k > 0) ? buf(ldv[k] * R * cd * pk) : nullptr;
+    if (f64lvl[k]) continue;       // contracted in FP64: no operand copies
     // A16: row (a + r z), K = al
     const long long lda = pad_k(r1, tf32);
     A16[k] = buf(r * n * lda);
@@ -232,6 +248,29 @@ void emit_sketch_op_tc(Builder& B, const DevTTO& H, ttc_batch* x, int t, const S
     std::vector<Bf16GemmDesc> g1, g2, g3;
     const long long n = x->dims[k], r = x->rk(t, k), r1 = x->rk(t, k + 1);
     const long long R = H.rks[k], R1 = H.rks[k + 1], g = sp.b[k + 1], cd = sp.b[k], pk = sp.p[k];
+    if (f64lvl[k]) {
+      OpEnvStep st{};
+      st.A = x->core(t, k); st.r = (int)r; st.xc = x->capr(t, k); st.r1 = (int)r1;
+      st.H = H.core(k); st.R = (int)R; st.R1 = (int)R1;
+      st.n = (int)n;
+      st.g = (int)g; st.cdim = (int)cd;
+      st.S = S[k]; st.s_k = 1; st.s_c = n * g;
+      st.V = W[k + 1];
+      st.W = W[k];
+      st.batch = (int)pk;
+      st.v_b = (k < N - 1) ? r1 * R1 * g : 0;
+      st.s_b = n * g * cd;
+      st.w_b = r * R * cd;
+      emit_op_env(B, {st});
+      if (k > 0) {                                   // the next (tensor-core) level's V operand
+        CvtDesc c{};
+        c.src = W[k]; c.dst = V16[k];
+        c.rows = r; c.cols = R * cd * pk; c.ss_i = 1; c.ss_j = r; c.ds_i = 1; c.ds_j = ldv[k]; c.alpha = 1.0;
+        B.cvt_bf16({c}, tf32);
+      }
+      B.release(mk);
+      continue;
+    }
     const long long ldt1 = pad_k(n * R1, tf32), ldt2 = pad_k(n * g, tf32), lda = pad_k(r1, tf32);
     const long long lds = pad_k(n * g, tf32), ldh = pad_k(n * R1, tf32);
     for (long long j = 0; j < pk; ++j) {

@@ -59,8 +59,10 @@ def test_operator_sketch_tf32_closer_than_bf16_with_blocks():
 @pytest.mark.parametrize("precision", ["bf16", "tf32"])
 def test_operator_rounding_mixed_precision_error_matches_fp64(precision):
     """Rounding H x without forming it, with a sketch of rank 30 against H x of rank up to 7*8: the
-    tensor-core sketch gives an error within 10 % of the FP64 sketch's, and the FP64 range finder
-    keeps the cores orthonormal."""
+    tensor-core sketch's error exceeds the FP64 sketch's by at most 1e-5 (the bound stated for the
+    mixed-precision paths; the levels whose right interface is structurally rank deficient are
+    contracted in FP64, which keeps the BF16 and TF32 results this close), and the FP64 range
+    finder keeps the cores orthonormal."""
     H, x = _case()
     rks = [1] + [30] * 9 + [1]
     Hx = o.tto_apply(H, x)
@@ -69,7 +71,7 @@ def test_operator_rounding_mixed_precision_error_matches_fp64(precision):
                                     precision=precision)
     assert ztc.ttv_rks == z64.ttv_rks
     e64, etc = rel(z64, Hx), rel(ztc, Hx)
-    assert etc <= 1.1 * e64 + 1e-12
+    assert etc <= e64 + 1e-5, (etc, e64)
     for c in ztc.ttv_vec[:-1]:
         Q = np.asarray(c).reshape(-1, c.shape[2], order="F")
         assert np.abs(Q.T @ Q - np.eye(Q.shape[1])).max() < 1e-12
