@@ -342,13 +342,13 @@ def other_configs(ttcuda, ctx, hbm_peak, stream):
                       "fp32": {"value": 1e3 / ms_g32, "unit": "gradients/s", "ms": ms_g32,
                                "variant": "FP32 cores and environments, FP32 accumulation",
                                "rel_diff_gradient_vs_fp64": gd / gn, "rel_diff_value_vs_fp64": abs(R32 - R64) / abs(R64)}}
-    # config 5 shapes: 48 sites, x of rank 512, operator-aware rounding to a rank-522 sketch (block_rks =
-    # 522) with the sketch contractions in BF16 on the tensor cores, FP32 accumulation, FP64 range
+    # config 5 shapes: 48 sites, x of rank 512, operator-aware rounding to rank 512 (block_rks = 512)
+    # with the sketch contractions in BF16 on the tensor cores, FP32 accumulation, FP64 range
     # finder and QR.  The 48-spin-orbital molecular MPO has rank ~2L^2+3L+2 = 1226 (L = 24 spatial
     # orbitals); its roundings need Householder QRs of ~4900 rows, beyond the QR kernel's 1536, so a
     # stand-in MPO of the same sites with ranks min(4^k, 4^(d-k), 192) and N(0,1)/sqrt(4 R_k) cores
     # takes its place here.
-    d5, R5, r5, s5 = 48, 192, 512, 522
+    d5, R5, r5, s5 = 48, 192, 512, 512      # block_rks = 512: every bond's sketch rank is 512
     g5 = np.random.default_rng(55)
     Rk = [min(4 ** min(k, d5 - k), R5) for k in range(d5 + 1)]
     H5 = ttcuda.TToperator(d5, [np.asfortranarray(g5.standard_normal((2, 2, Rk[k], Rk[k + 1])) / math.sqrt(4 * Rk[k + 1]))
@@ -383,6 +383,39 @@ def other_configs(ttcuda, ctx, hbm_peak, stream):
     return out
 
 
+# ------------------------------------------------------------------- kernel benchmarks
+def kernel_bench(reps):
+    """The tcgen05 sketch GEMM in isolation on the operator-sketch shapes of config 5 (x rank 512,
+    MPO rank 192 stand-in, sketch rank 512, n = 2: G1 M=1024 N=98304 K=512, G2 M=262144 N=384
+    K=384, G3 M=98304 N=512 K=1024) and on a square 8192^3, device-resident operands, CUDA events
+    on the library's stream; prints one JSON line."""
+    import ctypes as C
+    import torch  # noqa: F401  (initialises the device the way the main bench does)
+    import ttcuda
+    from ttcuda._lib import lib
+    lib.ttc_test_tc_gemm_bench.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.POINTER(C.c_double)]
+    lib.ttc_test_tc_gemm_bench.restype = C.c_int
+    ctx = ttcuda.Context(0)
+    peak, src = 1590.0, "fallback (MEASURED_PEAKS.json absent)"
+    try:
+        peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
+        src = "MEASURED_PEAKS.json bf16_tflops (measured burst)"
+    except Exception:
+        pass
+    shapes = {"G1": (1024, 98304, 512), "G2": (262144, 384, 384), "G3": (98304, 512, 1024), "square": (8192, 8192, 8192)}
+    out = {}
+    for tf32 in (0, 1):
+        for name, (m, n, k) in shapes.items():
+            ms = C.c_double()
+            ctx.check(lib.ttc_test_tc_gemm_bench(ctx.h, m, n, k, tf32, reps, C.byref(ms)))
+            tf = 2.0 * m * n * k / (ms.value / 1e3) / 1e12
+            out[("tf32:" if tf32 else "bf16:") + name] = {"m": m, "n": n, "k": k, "ms": ms.value, "tflops": tf,
+                                                          "frac_of_bf16_peak": tf / peak}
+    print(json.dumps({"kernel_bench": "gemm_bf16_tc_kernel", "peak_tflops": peak, "peak_source": src,
+                      "results": out}), flush=True)
+
+
 # ---------------------------------------------------------------------------- ours
 def main():
     ap = argparse.ArgumentParser()
@@ -392,7 +425,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-other-configs", action="store_true", help="skip the config 1, 2 and 4 lines")
+    ap.add_argument("--no-other-configs", action="store_true", help="skip the config 1, 2, 4 and 5 lines")
+    ap.add_argument("--kernel-bench", action="store_true",
+                    help="time the tcgen05 sketch GEMM alone on the config-5 shapes and exit")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -400,6 +435,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.kernel_bench:
+        kernel_bench(max(3, args.steps))
         return
 
     import torch

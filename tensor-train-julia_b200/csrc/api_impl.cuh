@@ -1,5 +1,6 @@
 // Host-level implementations behind the one-shot C entry points.
 #pragma once
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -45,6 +46,11 @@ void with_svd_retry(ttc_context* c, F&& run) {
     set_jacobi_max_sweeps(c, cap0);
   }
 }
+
+// A cached device batch of a one-shot entry point: the batch stored under `key`, or a new one
+// from `make` (the eight most recently used are kept; older ones are destroyed).
+ttc_batch* oneshot_batch(ttc_context* c, const std::string& key, const std::function<ttc_batch*()>& make);
+void oneshot_clear(ttc_context* c);
 
 struct BatchHolder {
   std::vector<ttc_batch*> v;

@@ -326,6 +326,32 @@ ttc_batch* batch_from_host(ttc_context* c, const ttc_ttv* x, const std::vector<i
   return b;
 }
 
+ttc_batch* oneshot_batch(ttc_context* c, const std::string& key, const std::function<ttc_batch*()>& make) {
+  auto& v = c->oneshot;
+  for (size_t i = 0; i < v.size(); ++i)
+    if (v[i].first == key) {
+      auto e = v[i];
+      v.erase(v.begin() + (long)i);
+      v.push_back(e);
+      return e.second;
+    }
+  ttc_batch* b = make();
+  v.emplace_back(key, b);
+  constexpr size_t kKeep = 8;
+  while (v.size() > kKeep) {
+    TTC_CUDA(cudaStreamSynchronize(c->stream));
+    ttc_batch* old = v.front().second;
+    v.erase(v.begin());
+    batch_destroy(old);            // drops the plans that name it as well
+  }
+  return b;
+}
+
+void oneshot_clear(ttc_context* c) {
+  for (auto& e : c->oneshot) batch_destroy(e.second);
+  c->oneshot.clear();
+}
+
 ttc_batch* batch_empty_like(ttc_context* c, int count, int N, const std::vector<long long>& dims,
                             const std::vector<int>& cap_per_tt) {
   std::vector<int> cp;
@@ -439,6 +465,10 @@ int ttc_destroy(ttc_context* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   c->plans.clear();
+  try {
+    oneshot_clear(c);
+  } catch (...) {
+  }
   for (void* p : {(void*)c->ws, c->d_stage, (void*)c->d_sk, (void*)c->d_flags, (void*)c->d_one}) region_remove(p);
   if (c->ws) cudaFree(c->ws);
   if (c->d_stage) cudaFree(c->d_stage);

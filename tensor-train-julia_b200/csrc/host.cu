@@ -19,13 +19,27 @@ void tt_rounding_host(ttc_context* c, const ttc_ttv* x, const ttc_round_opts& o,
   TTC_REQUIRE(o.direction == TTC_DIR_LEFT || o.direction == TTC_DIR_RIGHT, TTC_EARG,
               "Invalid direction. Use direction=:right or direction=:left");
   const bool rev = (o.direction == TTC_DIR_RIGHT);
-  BatchHolder H;
-  ttc_batch* xb = H.add(batch_from_host(c, x, nullptr, rev));
+  validate_ttv(x);
   const int N = x->N;
+  // the call's device batches are cached by shape: a repeated call uploads into the same memory
+  // and replays its captured plan
+  std::string shape = ":" + std::to_string(N) + (rev ? "r" : "l");
+  for (int k = 0; k < N; ++k) shape += "," + std::to_string(x->dims[k]);
+  for (int k = 0; k <= N; ++k) shape += "," + std::to_string(x->rks[k]);
+  ttc_batch* xb = oneshot_batch(c, "round.x" + shape, [&] {
+    std::vector<long long> dims(N);
+    for (int k = 0; k < N; ++k) dims[k] = x->dims[rev ? N - 1 - k : k];
+    std::vector<int> cp(N + 1);
+    for (int k = 0; k <= N; ++k) cp[k] = (int)x->rks[rev ? N - k : k];
+    return batch_create(c, 1, N, dims.data(), cp.data());
+  });
+  batch_upload_many(xb, 0, 1, x, rev);
   std::vector<int> cap(N + 1);
   if (is_left_orth(xb, 0)) for (int k = 0; k <= N; ++k) cap[k] = xb->rk(0, k);
   else cap = orth_left_ranks(xb, 0);
-  ttc_batch* yb = H.add(batch_create(c, 1, N, xb->dims.data(), cap.data()));
+  std::string cs = shape;
+  for (int v : cap) cs += "," + std::to_string(v);
+  ttc_batch* yb = oneshot_batch(c, "round.y" + cs, [&] { return batch_create(c, 1, N, xb->dims.data(), cap.data()); });
   ttc_round_opts lo = o;
   lo.direction = TTC_DIR_LEFT;
   with_svd_retry(c, [&] {

@@ -106,6 +106,10 @@ struct ttc_context {
   size_t sk_cap = 0;
   bool profiling = false;           // per-kernel-family event timing (ttc_set_profiling)
   int jacobi_max_sweeps = ttc::kJacobiDefaultSweeps;   // sweep cap of the one-sided Jacobi SVD
+  // device batches of the one-shot entry points (ttc_tt_rounding ...), reused by later calls of
+  // the same shape, most recently used last; reuse also lets the plan cache, which is keyed on
+  // batch identity, replay the captured plan
+  std::vector<std::pair<std::string, ttc_batch*>> oneshot;
 };
 
 struct ttc_batch {

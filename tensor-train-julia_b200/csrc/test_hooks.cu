@@ -63,6 +63,46 @@ int ttc_test_set_jacobi_max_sweeps(ttc_context* c, int sweeps) {
   }
 }
 
+// Device-resident timing of the tcgen05 GEMM C = A B^T (M x N, K; BF16 operands, or FP32 read as
+// TF32) for kernel benchmarks: operands filled on the device, `reps` launches of one plan timed
+// with events on the context stream after one warm-up launch; *ms_out = milliseconds per launch.
+int ttc_test_tc_gemm_bench(ttc_context* c, int m, int n, int k, int tf32, int reps, double* ms_out) {
+  return hook(c, [&] {
+    TTC_REQUIRE(m > 0 && n > 0 && k > 0 && reps > 0 && ms_out, TTC_EARG, "tc gemm bench: bad arguments");
+    const long long esz = tf32 ? 4 : 2, chunk = 16 / esz;
+    const long long ld = (k + chunk - 1) / chunk * chunk;
+    DevBuf dA((size_t)(m * ld * esz)), dB((size_t)(n * ld * esz)), dC((size_t)m * n * 4), dS((size_t)std::max(m, n) * ld * 8);
+    // operands: a smooth deterministic pattern converted from FP64 on the device
+    run_plan_once(c, [&](Builder& B) {
+      std::vector<PhiloxDesc> ph{{dS.as<double>(), (long long)std::max(m, n) * ld, 7ull, 0u, 0.1}};
+      B.philox(ph);
+      CvtDesc a{}, b{};
+      a.src = dS.as<double>(); a.dst = dA.p; a.rows = k; a.cols = m; a.ss_i = 1; a.ss_j = ld; a.ds_i = 1; a.ds_j = ld; a.alpha = 1.0;
+      b = a; b.dst = dB.p; b.cols = n;
+      B.cvt_bf16({a, b}, tf32 != 0);
+    });
+    std::string key = "tcbench:" + std::to_string(m) + ":" + std::to_string(n) + ":" + std::to_string(k);
+    Plan* p = get_plan(c, key, [&](Builder& B) {
+      Bf16GemmDesc d{};
+      d.m = m; d.n = n; d.k = k; d.m0 = m;
+      d.A = dA.p; d.lda = ld; d.B = dB.p; d.ldb = ld;
+      d.C32 = dC.as<float>(); d.c_i0 = 1; d.c_i1 = 0; d.c_j = m;
+      d.alpha = 1.0;
+      B.bf16gemm({d}, tf32 != 0);
+    });
+    run_plan(c, *p);
+    TTC_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    for (int i = 0; i < reps; ++i) run_plan(c, *p);
+    TTC_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    TTC_CUDA(cudaEventSynchronize(c->ev[1]));
+    float ms = 0.f;
+    TTC_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+    *ms_out = ms / reps;
+    TTC_CUDA(cudaStreamSynchronize(c->stream));
+    c->plans.erase(key);
+  });
+}
+
 // Builds a plan whose copy descriptor points `offset` bytes past the end of the context's
 // workspace: the host-side registry check refuses it (TTC_EINTERNAL) before any launch.
 int ttc_test_bad_descriptor(ttc_context* c, long long offset) {
