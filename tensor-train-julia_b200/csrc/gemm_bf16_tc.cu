@@ -1,28 +1,33 @@
 // Grouped BF16 or TF32 GEMM on the 5th-generation tensor cores (tcgen05, sm_100a), FP32
 // accumulation in tensor memory.  Used for the reverse-sketch contractions of
-// tt_recursive_sketch (src/sketches.jl:1602-1638) in the mixed-precision rounding:
+// tt_recursive_sketch (src/sketches.jl:1602-1638, :1648-1713) in the mixed-precision roundings:
 //   C(i, j) = alpha * sum_k A(i, k) * B(j, k),   A and B K-major, BF16 (kind::f16) or FP32
 //   read as TF32 (kind::tf32), row stride lda/ldb a multiple of 8 (BF16) or 4 (FP32)
 //   elements, K zero padded to that multiple.
-// Tile 128 x 128 x (128 bytes of K: 64 BF16 or 32 FP32), one CTA (4 warps) per output tile.
+// Tile 128 x 256 x (128 bytes of K: 64 BF16 or 32 FP32), one CTA (4 warps) per output tile; the
+// MMA's N is the tile's column count rounded up to 16, so narrow problems do not pay for 256.
 // Operand tiles are staged with cp.async into the 128-byte-swizzled K-major layout that the
-// UMMA shared-memory descriptors describe; one elected thread issues four tcgen05.mma per
-// tile (M=128, N=128, K=16 BF16 or K=8 TF32: 32 bytes of K each) and tcgen05.commit arrives
-// on an mbarrier; a two-stage ring overlaps the next tile's loads with the current MMAs.  The
-// epilogue reads the accumulator with tcgen05.ld (32x32b) and writes FP64 / FP32 outputs and
-// an operand-typed (BF16 or FP32) output with arbitrary (split) strides.
-// Every mbarrier wait is bounded: on timeout the kernel raises DFLAG_TIMEOUT, frees its
-// tensor memory and returns.
+// UMMA shared-memory descriptors describe, in a four-stage ring: while one elected thread issues
+// a stage's four tcgen05.mma (M=128, N<=256, 32 bytes of K each) and tcgen05.commit arrives on
+// the stage's mbarrier, the next three stages' loads are in flight.  The epilogue reads the
+// accumulator with tcgen05.ld (32x32b) and writes FP64 / FP32 outputs and an operand-typed (BF16
+// or FP32) output with arbitrary (split) row and column strides.
+// Every mbarrier wait is bounded (by a device-wide limit that a test may lower): on timeout the
+// kernel raises DFLAG_TIMEOUT, waits with the full limit for the MMAs it did issue, so that tensor
+// memory is never released under them, frees its tensor memory and returns.
 #include <cuda_bf16.h>
 
 #include "kernels.cuh"
 
 namespace ttc {
 namespace {
-constexpr int BM = 128, BN = 128, NT = 128, STAGES = 2;
-constexpr int TILE_BYTES = BM * 128;                    // 16 KB per operand tile (128 B of K per row)
-constexpr uint32_t TMEM_COLS = 128;
+constexpr int BM = 128, BN = 256, NT = 128, STAGES = 4;
+constexpr int A_TILE = BM * 128;                        // 16 KB (128 B of K per row)
+constexpr int B_TILE = BN * 128;                        // 32 KB
+constexpr int STAGE_BYTES = A_TILE + B_TILE;
+constexpr uint32_t TMEM_COLS = 256;
 constexpr long long WAIT_LIMIT = 1LL << 24;             // bounded mbarrier polls
+__device__ long long g_tc_wait_limit = WAIT_LIMIT;      // lowered only by a test hook
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -51,8 +56,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < WAIT_LIMIT; ++i)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+  for (long long i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -72,26 +77,26 @@ __device__ __forceinline__ uint64_t make_sdesc(uint32_t saddr) {
 // kind::f16, 2 = TF32 for kind::tf32; A and B always the same type), both K-major, N>>3 at bit
 // 17, M>>4 at bit 24.
 template <bool TF32>
-__host__ __device__ constexpr uint32_t idesc() {
-  return (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) | ((uint32_t)(BN >> 3) << 17) |
+__host__ __device__ constexpr uint32_t idesc(int n_mma) {
+  return (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) | ((uint32_t)(n_mma >> 3) << 17) |
          ((uint32_t)(BM >> 4) << 24);
 }
 
 template <bool TF32>
-__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t id, uint32_t accumulate) {
   if constexpr (TF32)
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc<true>()), "r"(accumulate)
+        "l"(adesc), "l"(bdesc), "r"(id), "r"(accumulate)
         : "memory");
   else
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc<false>()), "r"(accumulate)
+        "l"(adesc), "l"(bdesc), "r"(id), "r"(accumulate)
         : "memory");
 }
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
@@ -130,10 +135,9 @@ __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc*
   extern __shared__ __align__(1024) unsigned char dsm[];
   __shared__ uint64_t mbar[STAGES];
   __shared__ uint32_t tmem_base_sh;
-  // 1024-byte aligned operand ring
+  __shared__ int s_last;                   // last iteration whose MMAs were issued (-1: none)
+  // 1024-byte aligned operand ring: stage s holds A at s*STAGE_BYTES, B after it
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(dsm) + 1023) & ~uintptr_t(1023));
-  unsigned char* As = base;
-  unsigned char* Bs = base + STAGES * TILE_BYTES;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long long tile = blockIdx.x;
@@ -144,6 +148,10 @@ __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc*
   const int bm = (int)(local % tm), bn = (int)(local / tm);
   const int row0 = bm * BM, col0 = bn * BN;
   const int nk = (D.k + BK - 1) / BK;
+  const int ncols = min(BN, D.n - col0);
+  const int n_mma = (ncols + 15) & ~15;    // MMA N: the tile's columns rounded up to 16
+  const uint32_t id = idesc<TF32>(n_mma);
+  const long long wait_limit = g_tc_wait_limit;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
@@ -154,6 +162,7 @@ __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc*
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(smem_u32(&mbar[s]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_last = -1;
   }
   tc_fence_before();
   __syncthreads();
@@ -163,53 +172,70 @@ __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc*
   const char* Ag = reinterpret_cast<const char*>(D.A);
   const char* Bg = reinterpret_cast<const char*>(D.B);
 
-  // Each thread moves 8 of the 1024 16-byte chunks of each operand tile.
+  // A: 1024 16-byte chunks per tile (8 per thread); B: 8 chunks per row, n_mma rows
   auto load_stage = [&](int kt, int s) {
     const int k0 = kt * BK;
-    const uint32_t sa = smem_u32(As + s * TILE_BYTES), sb = smem_u32(Bs + s * TILE_BYTES);
+    const uint32_t sa = smem_u32(base + s * STAGE_BYTES), sb = sa + A_TILE;
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
-      const int idx = tid + NT * t;          // 0..1023
-      const int r = idx >> 3, c = idx & 7;   // row, 16-byte chunk within the 128-byte row
+      const int idx = tid + NT * t;
+      const int r = idx >> 3, c = idx & 7;
       const int kk = k0 + c * CH;
       const uint32_t off = (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
-      const int gi = row0 + r, gj = col0 + r;
+      const int gi = row0 + r;
       const bool va = (gi < D.m) && (kk < D.k);
-      const bool vb = (gj < D.n) && (kk < D.k);
       cp_async_16(sa + off, va ? (const void*)(Ag + ((long long)gi * D.lda + kk) * EB) : (const void*)Ag, va);
+    }
+    for (int idx = tid; idx < n_mma * 8; idx += NT) {
+      const int r = idx >> 3, c = idx & 7;
+      const int kk = k0 + c * CH;
+      const uint32_t off = (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
+      const int gj = col0 + r;
+      const bool vb = (gj < D.n) && (kk < D.k);
       cp_async_16(sb + off, vb ? (const void*)(Bg + ((long long)gj * D.ldb + kk) * EB) : (const void*)Bg, vb);
     }
     cp_async_commit();
   };
 
+  // prologue: stages 0 .. STAGES-2 in flight (an empty group keeps the group count uniform)
+#pragma unroll
+  for (int p = 0; p < STAGES - 1; ++p) {
+    if (p < nk) load_stage(p, p);
+    else cp_async_commit();
+  }
   bool ok = true;
-  load_stage(0, 0);
   for (int kt = 0; kt < nk; ++kt) {
-    const int s = kt & 1;
-    if (kt + 1 < nk) {
-      // stage s^1 was read by the MMAs of iteration kt-1
-      if (kt >= 1) ok = ok && mbar_wait(smem_u32(&mbar[s ^ 1]), (uint32_t)(((kt - 1) >> 1) & 1));
-      load_stage(kt + 1, s ^ 1);
-      cp_async_wait<1>();
+    const int s = kt % STAGES;
+    const int next = kt + STAGES - 1;
+    if (next < nk) {
+      // the stage of `next` was read by the MMAs of iteration kt - 1
+      if (kt >= 1) ok = ok && mbar_wait(smem_u32(&mbar[next % STAGES]), (uint32_t)(((kt - 1) / STAGES) & 1), wait_limit);
+      load_stage(next, next % STAGES);
     } else {
-      cp_async_wait<0>();
+      cp_async_commit();
     }
+    cp_async_wait<STAGES - 1>();            // this iteration's stage has landed
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     if (tid == 0 && ok) {
       tc_fence_after();
-      const uint32_t sa = smem_u32(As + s * TILE_BYTES), sb = smem_u32(Bs + s * TILE_BYTES);
+      const uint32_t sa = smem_u32(base + s * STAGE_BYTES), sb = sa + A_TILE;
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {   // 32 bytes of K per MMA
-        umma<TF32>(tmem, make_sdesc(sa + kk * 32), make_sdesc(sb + kk * 32), (kt > 0 || kk > 0) ? 1u : 0u);
-      }
+      for (int kk = 0; kk < 4; ++kk)        // 32 bytes of K per MMA
+        umma<TF32>(tmem, make_sdesc(sa + kk * 32), make_sdesc(sb + kk * 32), id, (kt > 0 || kk > 0) ? 1u : 0u);
       umma_commit(smem_u32(&mbar[s]));
+      s_last = kt;
     }
     __syncthreads();
   }
-  if (nk > 0) ok = ok && mbar_wait(smem_u32(&mbar[(nk - 1) & 1]), (uint32_t)(((nk - 1) >> 1) & 1));
+  cp_async_wait<0>();
+  if (nk > 0) ok = ok && mbar_wait(smem_u32(&mbar[(nk - 1) % STAGES]), (uint32_t)(((nk - 1) / STAGES) & 1), wait_limit);
   ok = __syncthreads_and(ok) != 0;
-  if (!ok && nk > 0) mbar_wait(smem_u32(&mbar[(nk - 1) & 1]), (uint32_t)(((nk - 1) >> 1) & 1));  // drain, bounded
+  if (!ok) {
+    // drain with the full limit: the MMAs that were issued finish before tensor memory is freed
+    const int last = s_last;
+    if (last >= 0) mbar_wait(smem_u32(&mbar[last % STAGES]), (uint32_t)((last / STAGES) & 1), WAIT_LIMIT);
+  }
   tc_fence_after();
   if (!ok) {
     if (tid == 0) atomicOr(flags, DFLAG_TIMEOUT);
@@ -218,7 +244,7 @@ __global__ void __launch_bounds__(NT, 1) gemm_bf16_tc_kernel(const Bf16GemmDesc*
     const int row = row0 + warp * 32 + lane;
     const long long roff64 = (long long)(row % D.m0) * D.c_i0 + (long long)(row / D.m0) * D.c_i1;
     const long long roff16 = (long long)(row % D.m0) * D.h_i0 + (long long)(row / D.m0) * D.h_i1;
-    for (int c0 = 0; c0 < BN; c0 += 16) {
+    for (int c0 = 0; c0 < n_mma; c0 += 16) {
       float v[16];
       if (nk > 0) tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
       else {
@@ -260,7 +286,7 @@ long long bf16_gemm_tiles(const Bf16GemmDesc& d) {
 namespace {
 template <bool TF32>
 void launch_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags) {
-  const int smem = STAGES * 2 * TILE_BYTES + 1024;
+  const int smem = STAGES * STAGE_BYTES + 1024;
   static PerDeviceOnce attr_once;
   int dev = 0;
   TTC_CUDA(cudaGetDevice(&dev));
@@ -271,6 +297,11 @@ void launch_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_
   TTC_CHECK_LAUNCH();
 }
 }  // namespace
+
+void set_tc_wait_limit(long long polls) {
+  TTC_REQUIRE(polls >= 1, TTC_EARG, "the tensor-core wait limit must be at least 1");
+  TTC_CUDA(cudaMemcpyToSymbol(g_tc_wait_limit, &polls, sizeof(polls)));
+}
 
 void launch_gemm_bf16_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, cudaStream_t s, int* d_flags,
                          bool tf32) {

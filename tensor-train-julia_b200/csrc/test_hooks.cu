@@ -63,6 +63,12 @@ int ttc_test_set_jacobi_max_sweeps(ttc_context* c, int sweeps) {
   }
 }
 
+// Sets the poll limit of the tensor-core GEMM's bounded mbarrier waits on the context's device
+// (default 2^24), so that a test can make the waits run out on purpose.
+int ttc_test_set_tc_wait_limit(ttc_context* c, long long polls) {
+  return hook(c, [&] { set_tc_wait_limit(polls); });
+}
+
 // Device-resident timing of the tcgen05 GEMM C = A B^T (M x N, K; BF16 operands, or FP32 read as
 // TF32) for kernel benchmarks: operands filled on the device, `reps` launches of one plan timed
 // with events on the context stream after one warm-up launch; *ms_out = milliseconds per launch.

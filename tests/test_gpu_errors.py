@@ -8,7 +8,10 @@ context checked to stay usable afterwards:
   the library's single retry at four times the cap (the reference retries a failed gesdd with QR
   iteration, src/tt_rounding.jl:191-195), which then succeeds and is counted in ttc_stats;
 * a kernel descriptor pointing outside every device allocation of the library -> TTC_EINTERNAL
-  from the host-side registry check, before anything is launched.
+  from the host-side registry check, before anything is launched;
+* the tensor-core GEMM's bounded mbarrier waits lowered to one poll through a test hook so that
+  they run out -> DFLAG_TIMEOUT, reported as TTC_EINTERNAL after the kernel drained the MMAs it
+  issued and returned.
 """
 import ctypes as C
 
@@ -26,6 +29,10 @@ lib.ttc_test_set_jacobi_max_sweeps.argtypes = [C.c_void_p, C.c_int]
 lib.ttc_test_set_jacobi_max_sweeps.restype = C.c_int
 lib.ttc_test_bad_descriptor.argtypes = [C.c_void_p, C.c_longlong]
 lib.ttc_test_bad_descriptor.restype = C.c_int
+lib.ttc_test_set_tc_wait_limit.argtypes = [C.c_void_p, C.c_longlong]
+lib.ttc_test_set_tc_wait_limit.restype = C.c_int
+lib.ttc_test_tc_gemm_bench.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+lib.ttc_test_tc_gemm_bench.restype = C.c_int
 
 
 @pytest.fixture()
@@ -33,6 +40,7 @@ def ctx():
     c = ttcuda.get_context()
     yield c
     c.check(lib.ttc_test_set_jacobi_max_sweeps(c.h, 40))
+    c.check(lib.ttc_test_set_tc_wait_limit(c.h, 1 << 24))
 
 
 def _still_usable():
@@ -102,3 +110,21 @@ def test_descriptor_outside_allocations_is_refused_before_launch(ctx):
     assert st == 7                                   # TTC_EINTERNAL
     assert b"outside device allocations" in lib.ttc_last_error(ctx.h)
     _still_usable()
+
+
+def test_tensor_core_wait_timeout_is_reported_and_context_recovers(ctx):
+    """The tcgen05 GEMM's mbarrier waits lowered to a single poll: a GEMM with 128 K-steps cannot
+    keep up, its waits run out, the kernel flags the timeout, waits (with the full limit) for the
+    MMAs it issued, frees its tensor memory and returns; the host reports TTC_EINTERNAL.  With the
+    limit restored the same GEMM and a BF16-sketch rounding run normally."""
+    ms = C.c_double()
+    ctx.check(lib.ttc_test_set_tc_wait_limit(ctx.h, 1))
+    st = lib.ttc_test_tc_gemm_bench(ctx.h, 256, 512, 8192, 0, 2, C.byref(ms))
+    assert st == 7                                   # TTC_EINTERNAL
+    assert b"bounded device wait" in lib.ttc_last_error(ctx.h)
+    ctx.check(lib.ttc_test_set_tc_wait_limit(ctx.h, 1 << 24))
+    ctx.check(lib.ttc_test_tc_gemm_bench(ctx.h, 256, 512, 8192, 0, 2, C.byref(ms)))
+    assert ms.value > 0
+    x = decaying_tt((2,) * 10, o.r_and_d_to_rks([1] + [12] * 9 + [1], (2,) * 10), seed=8, decay_per=3.0)
+    got = ttcuda.ttrand_rounding(to_dev(x), [1] + [20] * 9 + [1], orthogonal=False, seed=3, precision="bf16")
+    assert rel(got, x) < 1e-10
