@@ -366,6 +366,11 @@ def other_configs(ttcuda, ctx, hbm_peak, stream):
     # 2048-row QR; the BF16/FP64 difference is far above the expansion's cancellation level
     aa, ab, bb = ttcuda.dot(z5d, z5d), ttcuda.dot(z5d, z5b), ttcuda.dot(z5b, z5b)
     rel5 = math.sqrt(max(0.0, aa - 2.0 * ab + bb) / aa)
+    # a randomized rounding is an orthogonal projection of H x (left-orthonormal cores), so <z, H x>
+    # = ||z||^2 is the energy it captures; in this heavy compression (H x has rank up to 98304)
+    # two sketches give different projections, and the captured energies compare their quality
+    cap_b = ttcuda.dot_operator(z5b, H5, x5) / math.sqrt(bb)
+    cap_d = ttcuda.dot_operator(z5d, H5, x5) / math.sqrt(aa)
     ctx.set_profiling(True)
     run5("bf16")
     prof5 = ctx.kernel_profile()
@@ -380,6 +385,8 @@ def other_configs(ttcuda, ctx, hbm_peak, stream):
         "variant": "BF16 operator sketch (tcgen05), FP32 accumulation; FP64 range finder, QR and projections",
         "fp64": {"value": 1e3 / ms5d, "unit": "roundings/s", "ms": ms5d},
         "rel_diff_vs_fp64": rel5, "ranks_identical_fp64": z5b.ttv_rks == z5d.ttv_rks,
+        "captured_norm_bf16": cap_b, "captured_norm_fp64": cap_d,
+        "captured_norm_ratio_bf16_over_fp64": cap_b / cap_d,
         "tcgen05_sketch": {"ms": tc[0], "launches": tc[1], "tflop": tc[2] / 1e12,
                            "tflops": (tc[2] / (tc[0] / 1e3) / 1e12) if tc[0] > 0 else None},
         "profile_ms": {k: round(v[0], 3) for k, v in prof5.items() if v[1]}}

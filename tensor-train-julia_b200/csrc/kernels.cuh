@@ -143,7 +143,7 @@ void launch_gemm_bf16_tc(const Bf16GemmDesc* d, int nd, long long total_tiles, c
                          bool tf32 = false);
 long long bf16_gemm_tiles(const Bf16GemmDesc& d);
 // Poll limit of the tensor-core GEMM's mbarrier waits on the current device (default 2^24); tests
-// lower it to make a wait run out on purpose.
+// set 0 to make the waits give up on purpose.
 void set_tc_wait_limit(long long polls);
 
 }  // namespace ttc

@@ -9,8 +9,7 @@ context checked to stay usable afterwards:
   iteration, src/tt_rounding.jl:191-195), which then succeeds and is counted in ttc_stats;
 * a kernel descriptor pointing outside every device allocation of the library -> TTC_EINTERNAL
   from the host-side registry check, before anything is launched;
-* the tensor-core GEMM's bounded mbarrier waits lowered to one poll through a test hook so that
-  they run out -> DFLAG_TIMEOUT, reported as TTC_EINTERNAL after the kernel drained the MMAs it
+* the tensor-core GEMM's bounded mbarrier waits set to give up at once through a test hook -> DFLAG_TIMEOUT, reported as TTC_EINTERNAL after the kernel drained the MMAs it
   issued and returned.
 """
 import ctypes as C
@@ -113,12 +112,13 @@ def test_descriptor_outside_allocations_is_refused_before_launch(ctx):
 
 
 def test_tensor_core_wait_timeout_is_reported_and_context_recovers(ctx):
-    """The tcgen05 GEMM's mbarrier waits lowered to a single poll: a GEMM with 128 K-steps cannot
-    keep up, its waits run out, the kernel flags the timeout, waits (with the full limit) for the
-    MMAs it issued, frees its tensor memory and returns; the host reports TTC_EINTERNAL.  With the
-    limit restored the same GEMM and a BF16-sketch rounding run normally."""
+    """The tcgen05 GEMM's mbarrier wait limit set to zero polls (one try_wait may itself block for a
+    while, so a limit of one is not certain to run out): every wait of a GEMM with 128 K-steps
+    gives up, the kernel flags the timeout, waits with the full limit for the MMAs it issued,
+    frees its tensor memory and returns; the host reports TTC_EINTERNAL.  With the limit restored
+    the same GEMM and a BF16-sketch rounding run normally."""
     ms = C.c_double()
-    ctx.check(lib.ttc_test_set_tc_wait_limit(ctx.h, 1))
+    ctx.check(lib.ttc_test_set_tc_wait_limit(ctx.h, 0))
     st = lib.ttc_test_tc_gemm_bench(ctx.h, 256, 512, 8192, 0, 2, C.byref(ms))
     assert st == 7                                   # TTC_EINTERNAL
     assert b"bounded device wait" in lib.ttc_last_error(ctx.h)
