@@ -510,6 +510,91 @@ __global__ void __launch_bounds__(NT, RMAX <= 8 ? 2 : 1)
   }
 }
 
+// Small problems (m, n <= 32, no W): one warp per problem, lane j holding column j in
+// registers.  A round of the circle method pairs the columns; the two lanes of a pair exchange
+// their columns by shuffles and both compute alpha, beta, gamma with the same operations in the
+// same order (so both find the same rotation bit for bit), each updating its own column.  No
+// barrier is needed, which is what bounds the cluster kernel on these sizes.  Same rotation, zero
+// threshold and convergence rule (a sweep without rotations) as the cluster kernel.
+__global__ void __launch_bounds__(128) jacobi_small_kernel(const JacobiDesc* __restrict__ descs, int count, int* flags,
+                                                          int max_sweeps) {
+  const int lane = threadIdx.x & 31;
+  const int prob = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (prob >= count) return;                        // uniform within the warp
+  const JacobiDesc D = descs[prob];
+  if (D.m <= 0 || D.n <= 0) return;
+  const int m = max(1, dev_bound(D.m, D.m_dev, D.m_mult)), n = D.n;
+  double x[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) x[i] = (lane < n && i < m) ? D.X[(long long)lane * D.ldx + i] : 0.0;
+  double nrm = 0.0;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) nrm = fma(x[i], x[i], nrm);
+  const double fro2 = warp_sum(nrm);
+  RotCfg q;
+  {
+    const double tol = jac_tol(D.m);
+    int e2 = 0;
+    if (fro2 > 0.0 && isfinite(fro2)) { frexp(fro2, &e2); e2 = (e2 + 1) & ~1; }
+    q.sc = (fro2 > 0.0 && isfinite(fro2)) ? ldexp(1.0, -e2) : 1.0;
+    q.tol2 = tol * tol;
+    q.zthr = q.tol2 * fro2 * q.sc;
+  }
+  const int ne = n + (n & 1);
+  bool converged = false;
+  int sweep = 0;
+  for (; sweep < max_sweeps && !converged; ++sweep) {
+    bool any = false;
+    for (int rd = 0; rd < ne - 1; ++rd) {
+      // this lane's position in the round, and its partner column
+      int pos = 0;
+      if (lane != 0) pos = ((lane - 1 - rd) % (ne - 1) + (ne - 1)) % (ne - 1) + 1;
+      const int partner = rr_player(ne - 1 - pos, rd, ne);
+      const bool act = lane < n && partner < n;
+      const int src = act ? partner : lane;
+      const bool low = lane < partner;
+      double a = 0.0, b = 0.0, g = 0.0;            // alpha (low column), beta (high), gamma
+      double y[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        y[i] = __shfl_sync(0xffffffffu, x[i], src);
+        const double lo = low ? x[i] : y[i], hi = low ? y[i] : x[i];
+        a = fma(lo, lo, a);
+        b = fma(hi, hi, b);
+        g = fma(lo, hi, g);
+      }
+      const Rot R = act ? make_rot(a, b, g, q) : Rot{1.0, 0.0, false};
+      if (R.apply) {
+        any = true;
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          x[i] = low ? (R.c * x[i] - R.s * y[i]) : fma(R.s, y[i], R.c * x[i]);
+      }
+    }
+    converged = !__any_sync(0xffffffffu, any);
+  }
+  if (!converged && lane == 0) atomicOr(flags, DFLAG_JACOBI_NOCONV);
+  if (D.info && lane == 0) *D.info = converged ? sweep : -sweep;
+  double c2 = 0.0;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) c2 = fma(x[i], x[i], c2);
+  const double sg = sqrt(c2);
+  if (lane < n) {
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+      if (i < m) D.X[(long long)lane * D.ldx + i] = x[i];
+    D.sigma[lane] = sg;
+  }
+  // ranking by decreasing value (NaN last, ties by index), as in the cluster kernel
+  const double key = (lane < n) ? ((sg == sg) ? sg : -1.0) : -2.0;
+  int rank = 0;
+  for (int j = 0; j < n; ++j) {
+    const double w = __shfl_sync(0xffffffffu, key, j);
+    rank += (w > key) || (w == key && j < lane);
+  }
+  if (lane < n) D.perm[rank] = lane;
+}
+
 // Problem order of a launch: by decreasing size m x n^2, m the rows left by the device bound and
 // n the columns (at most m when bounded: the bounded factor is square), ties by index.
 __global__ void jacobi_order_kernel(const JacobiDesc* __restrict__ descs, int count, int* __restrict__ order) {
@@ -605,6 +690,11 @@ void launch_jacobi(const JacobiDesc* d_descs, int count, int max_m, int max_n, b
   const int bw = jacobi_bw(max_m, max_n, accw, &smem);
   TTC_REQUIRE(smem <= 200 * 1024, TTC_EDIM, "jacobi: matrix too large for the shared-memory blocks");
   if (count > kJacobiOrderMax) order = nullptr;
+  if (!accw && max_m <= 32 && max_n <= 32) {       // every problem fits one warp's registers
+    jacobi_small_kernel<<<(unsigned)((count + 3) / 4), 128, 0, s>>>(d_descs, count, d_flags, max_sweeps);
+    TTC_CHECK_LAUNCH();
+    return;
+  }
   if (max_m <= 256) launch_jacobi_t<8>(d_descs, count, max_n, bw, smem, s, d_flags, order, max_sweeps);
   else launch_jacobi_t<16>(d_descs, count, max_n, bw, smem, s, d_flags, order, max_sweeps);
 }

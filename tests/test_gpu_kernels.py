@@ -105,7 +105,8 @@ def test_householder_qr(ctx, m, n):
     assert np.allclose(np.tril(R, -1), 0.0)
 
 
-@pytest.mark.parametrize("m,n,accw", [(1, 1, 0), (6, 6, 0), (32, 32, 0), (40, 40, 0), (64, 64, 0), (96, 80, 0),
+@pytest.mark.parametrize("m,n,accw", [(1, 1, 0), (6, 6, 0), (17, 17, 0), (32, 9, 0), (32, 32, 0), (40, 40, 0),
+                                      (64, 64, 0), (96, 80, 0),
                                       (256, 256, 0), (384, 384, 0), (512, 512, 0), (10, 4, 1), (64, 64, 1)])
 def test_jacobi(ctx, m, n, accw):
     g = np.random.default_rng(m * 7 + n)
@@ -184,3 +185,27 @@ def test_tf32_tcgen05_gemm(ctx, m, n, k):
     worst = np.unravel_index(np.argmax(ratio), ratio.shape)
     assert ratio.max() <= 1.0, f"worst element {worst}: got {got[worst]}, ref {ref[worst]}, bound {bound[worst]}"
     assert np.linalg.norm(got - ref) <= 2e-3 * np.linalg.norm(ref)
+
+
+def test_jacobi_small_rank_deficient(ctx):
+    """Sizes <= 32 run one problem per warp: a rank-16 24 x 24 factor (8 numerically zero columns
+    after mixing) converges, the zero singular values come out at the rounding level and the
+    others match."""
+    g = np.random.default_rng(5)
+    m = n = 24
+    U, _ = np.linalg.qr(g.standard_normal((m, n)))
+    V, _ = np.linalg.qr(g.standard_normal((n, n)))
+    s = np.concatenate([10.0 ** (-np.arange(16) / 4.0), np.zeros(8)])
+    X = (U * s) @ V.T
+    Xf = X.ravel(order="F").copy()
+    W = np.zeros(n * n)
+    sig = np.zeros(n)
+    perm = np.zeros(n, dtype=np.int32)
+    sweeps = np.zeros(1, dtype=np.int32)
+    ctx.check(lib.ttc_test_jacobi(ctx.h, m, n, ptr(Xf), 0, ptr(W), ptr(sig), perm.ctypes.data_as(PI),
+                                  sweeps.ctypes.data_as(PI)))
+    assert sweeps[0] > 0
+    ss = sig[perm]
+    assert sorted(perm.tolist()) == list(range(n))
+    assert np.allclose(ss[:16], s[:16], rtol=1e-10, atol=1e-14)
+    assert np.all(ss[16:] <= 1e-13)
