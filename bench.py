@@ -376,6 +376,7 @@ def other_configs(ttcuda, ctx, hbm_peak, stream):
     prof5 = ctx.kernel_profile()
     ctx.set_profiling(False)
     tc = prof5["gemm_bf16_tcgen05"]
+    gf5 = prof5["gemm_f64"]
     out["config5_shapes"] = {
         "workload": f"operator-aware ttrand_rounding([1.0], H, [x], rks): d=48, n=2, x rank {r5} (N(0,1), "
                     f"normalised), sketch rank {s5} (block_rks = {s5}, Gaussian), H a stand-in MPO of ranks "
@@ -389,6 +390,8 @@ def other_configs(ttcuda, ctx, hbm_peak, stream):
         "captured_norm_ratio_bf16_over_fp64": cap_b / cap_d,
         "tcgen05_sketch": {"ms": tc[0], "launches": tc[1], "tflop": tc[2] / 1e12,
                            "tflops": (tc[2] / (tc[0] / 1e3) / 1e12) if tc[0] > 0 else None},
+        "gemm_f64": {"ms": gf5[0], "launches": gf5[1], "tflop": gf5[2] / 1e12,
+                     "tflops": (gf5[2] / (gf5[0] / 1e3) / 1e12) if gf5[0] > 0 else None},
         "profile_ms": {k: round(v[0], 3) for k, v in prof5.items() if v[1]}}
     return out
 

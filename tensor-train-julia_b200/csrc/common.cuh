@@ -64,6 +64,13 @@ struct GemmDesc {
   // rank written by an earlier kernel): output columns >= *n_dev are B columns known to be zero,
   // so their tiles store zeros (beta == 0) or are skipped (beta != 0) without the product.
   const int* n_dev;
+  // Split-K (FP64 kernel only; set by the planner): ksplit > 1 CTAs share each output tile, each
+  // over a contiguous range of K; they leave their partial tiles in ws, and the last to finish
+  // (counted in cnt, one zeroed counter per output tile, reset by that CTA) adds them up in split
+  // order, so the result does not depend on which CTA finishes last.
+  int ksplit;
+  double* ws;
+  unsigned* cnt;
 };
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }

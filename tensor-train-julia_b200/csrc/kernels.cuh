@@ -9,6 +9,10 @@ void launch_gemm_f64(const GemmDesc* d_descs, int nd, long long total_tiles, cud
 // ---- the same problems with float data in A, B and C, FP32 accumulation (gemm_f32.cu)
 void launch_gemm_f32(const GemmDesc* d_descs, int nd, long long total_tiles, cudaStream_t s);
 long long gemm_tiles(const GemmDesc& d);
+// Split-K count for one FP64 problem of a launch of launch_tiles output tiles on nsm SMs (1: no
+// split), and the partial-tile workspace (doubles) a split problem needs.
+int gemm_pick_ksplit(const GemmDesc& d, long long launch_tiles, int nsm);
+long long gemm_split_ws_doubles(const GemmDesc& d);
 
 // Device-side size bound: min(cap, mult * *p) when p is given (a rank that an earlier kernel of
 // the same plan wrote), else cap.  Rows or columns beyond the bound are exactly zero in the

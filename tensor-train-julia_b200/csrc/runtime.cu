@@ -382,16 +382,33 @@ const int* Builder::const_ints(const std::vector<int>& v) {
 }
 void Builder::gemm(std::vector<GemmDesc> v) {
   std::vector<GemmDesc> w;
+  long long out_tiles = 0;
+  for (auto& d : v) {
+    d.ksplit = 1; d.ws = nullptr; d.cnt = nullptr;
+    out_tiles += gemm_tiles(d);
+  }
+  const int nsm = current_sm_count();
   long long t = 0;
   for (auto& d : v) {
-    const long long n = gemm_tiles(d);
-    if (n == 0) continue;
+    if (gemm_tiles(d) == 0) continue;
     if (d.m0 <= 0) d.m0 = std::max(d.m, 1);
     if (d.n0 <= 0) d.n0 = std::max(d.n, 1);
     if (d.k0e <= 0) d.k0e = std::max(d.k, 1);
     if (wsbase) check_gemm(d);
+    const long long tiles_out = gemm_tiles(d);
+    d.ksplit = gemm_pick_ksplit(d, out_tiles, nsm);
+    if (d.ksplit > 1) {
+      d.ws = wd((size_t)gemm_split_ws_doubles(d));
+      // one counter per output tile, zero in the plan blob; the kernel leaves them zero
+      const size_t o = plan->push(std::vector<unsigned>((size_t)tiles_out, 0u));
+      d.cnt = reinterpret_cast<unsigned*>(blob_base + o);
+      if (wsbase) {
+        region_check(d.ws, sizeof(double) * (size_t)gemm_split_ws_doubles(d), "gemm split-K partials");
+        region_check(d.cnt, sizeof(unsigned) * (size_t)tiles_out, "gemm split-K counters");
+      }
+    }
     d.tile_start = t;
-    t += n;
+    t += gemm_tiles(d);
     w.push_back(d);
   }
   if (w.empty()) return;

@@ -127,16 +127,24 @@ int ttc_test_bad_descriptor(ttc_context* c, long long offset) {
   });
 }
 
-// C = alpha * A * B + beta * C with split strides (a_str = {i0, i1, k0, k1, b}, ...).
-int ttc_test_gemm(ttc_context* c, int m, int n, int k, int batch, int m0, int n0, int k0e, const double* A,
-                  long long a_len, const long long* as, const double* Bh, long long b_len, const long long* bs,
-                  double* Ch, long long c_len, const long long* cs, double alpha, double beta) {
+// C = alpha * A * B + beta * C with split strides (a_str = {i0, i1, k0, k1, b}, ...), the plan
+// run `runs` times (with beta == 0 every run writes the same C; the repeats check that the
+// split-K tile counters are left zero for the next launch).  *ksplit_out (when given) receives
+// the split count the planner chose.
+int ttc_test_gemm_runs(ttc_context* c, int m, int n, int k, int batch, int m0, int n0, int k0e, const double* A,
+                       long long a_len, const long long* as, const double* Bh, long long b_len, const long long* bs,
+                       double* Ch, long long c_len, const long long* cs, double alpha, double beta, int runs,
+                       int* ksplit_out) {
   return hook(c, [&] {
+    TTC_REQUIRE(runs >= 1 && (runs == 1 || beta == 0.0), TTC_EARG, "repeated runs need beta == 0");
     DevBuf dA(a_len * 8), dB(b_len * 8), dC(c_len * 8);
     TTC_CUDA(cudaMemcpy(dA.p, A, a_len * 8, cudaMemcpyHostToDevice));
     TTC_CUDA(cudaMemcpy(dB.p, Bh, b_len * 8, cudaMemcpyHostToDevice));
     TTC_CUDA(cudaMemcpy(dC.p, Ch, c_len * 8, cudaMemcpyHostToDevice));
-    run_plan_once(c, [&](Builder& B) {
+    static unsigned long long serial = 0;
+    const std::string key = "hook-gemm:" + std::to_string(++serial);
+    int ks = 1;
+    Plan* p = get_plan(c, key, [&](Builder& B) {
       GemmDesc d{};
       d.m = m; d.n = n; d.k = k; d.batch = batch; d.m0 = m0; d.n0 = n0; d.k0e = k0e;
       d.A = dA.as<double>(); d.a_i0 = as[0]; d.a_i1 = as[1]; d.a_k0 = as[2]; d.a_k1 = as[3]; d.a_b = as[4];
@@ -144,9 +152,21 @@ int ttc_test_gemm(ttc_context* c, int m, int n, int k, int batch, int m0, int n0
       d.C = dC.as<double>(); d.c_i0 = cs[0]; d.c_i1 = cs[1]; d.c_j0 = cs[2]; d.c_j1 = cs[3]; d.c_b = cs[4];
       d.alpha = alpha; d.beta = beta;
       B.gemm({d});
+      ks = gemm_pick_ksplit(d, gemm_tiles(d), current_sm_count());
     });
+    for (int r = 0; r < runs; ++r) run_plan(c, *p);
+    TTC_CUDA(cudaStreamSynchronize(c->stream));
+    c->plans.erase(key);
+    if (ksplit_out) *ksplit_out = ks;
     TTC_CUDA(cudaMemcpy(Ch, dC.p, c_len * 8, cudaMemcpyDeviceToHost));
   });
+}
+
+int ttc_test_gemm(ttc_context* c, int m, int n, int k, int batch, int m0, int n0, int k0e, const double* A,
+                  long long a_len, const long long* as, const double* Bh, long long b_len, const long long* bs,
+                  double* Ch, long long c_len, const long long* cs, double alpha, double beta) {
+  return ttc_test_gemm_runs(c, m, n, k, batch, m0, n0, k0e, A, a_len, as, Bh, b_len, bs, Ch, c_len, cs, alpha, beta,
+                            1, nullptr);
 }
 
 // Householder QR of A (m x n, col-major): Q (m x K), R (K x n).

@@ -85,6 +85,68 @@ def test_gemm_transposed_and_split(ctx):
     assert np.allclose(got, ref, rtol=1e-13, atol=1e-12)
 
 
+lib.ttc_test_gemm_runs.argtypes = lib.ttc_test_gemm.argtypes + [C.c_int, PI]
+
+
+def ref_gemm_vec(m, n, k, batch, m0, n0, k0e, A, ast, B, bst, Cm, cst, alpha, beta):
+    """ref_gemm with numpy index arrays (for long K)."""
+    out = Cm.copy()
+    i, j, kk = np.arange(m), np.arange(n), np.arange(k)
+    ko_a = (kk % k0e) * ast[2] + (kk // k0e) * ast[3]
+    ko_b = (kk % k0e) * bst[0] + (kk // k0e) * bst[1]
+    for b in range(batch):
+        Am = A[((i % m0) * ast[0] + (i // m0) * ast[1] + b * ast[4])[:, None] + ko_a[None, :]]
+        Bm = B[ko_b[:, None] + ((j % n0) * bst[2] + (j // n0) * bst[3] + b * bst[4])[None, :]]
+        ic = ((i % m0) * cst[0] + (i // m0) * cst[1] + b * cst[4])[:, None] + ((j % n0) * cst[2] + (j // n0) * cst[3])[None, :]
+        out[ic] = alpha * (Am @ Bm) + (beta * Cm[ic] if beta != 0 else 0.0)
+    return out
+
+
+@pytest.mark.parametrize("m,n,k,beta", [(70, 65, 3000, 0.0), (130, 3, 4100, 0.0), (64, 64, 1024, 0.0),
+                                        (70, 65, 3000, 2.0), (200, 150, 700, 0.0)])
+def test_gemm_split_k(ctx, m, n, k, beta):
+    """Few output tiles and long K: the planner splits K over several CTAs per tile, the last of
+    which adds the partial tiles in split order; three runs of one plan (beta == 0) check that
+    the tile counters are left zero for the next launch."""
+    g = np.random.default_rng(m + n + k)
+    A = g.standard_normal((m, k))
+    B = g.standard_normal((k, n))
+    Cm = g.standard_normal((m, n))
+    Af, Bf, Cf = A.ravel(order="F").copy(), B.ravel(order="F").copy(), Cm.ravel(order="F").copy()
+    a_s, ap = lptr([1, 0, m, 0, 0])
+    b_s, bp = lptr([1, 0, k, 0, 0])
+    c_s, cp = lptr([1, 0, m, 0, 0])
+    ks = C.c_int(0)
+    runs = 3 if beta == 0.0 else 1
+    ctx.check(lib.ttc_test_gemm_runs(ctx.h, m, n, k, 1, m, n, k, ptr(Af), Af.size, ap, ptr(Bf), Bf.size, bp, ptr(Cf),
+                                     Cf.size, cp, 0.5, beta, runs, C.byref(ks)))
+    want = 0.5 * A @ B + beta * Cm
+    assert ks.value > 1 or (m, n, k) == (200, 150, 700)
+    assert np.abs(Cf.reshape((m, n), order="F") - want).max() <= 1e-12 * np.abs(want).max()
+
+
+def test_gemm_split_k_mixed_radix_batched(ctx):
+    """Split K over a K index of two strides (k0e = 7) with split rows and columns and a batch."""
+    g = np.random.default_rng(8)
+    m, n, k, batch, m0, n0, k0e = 12, 9, 2100, 3, 4, 3, 7
+    ast = [7, 29, 1, 97, 70000]
+    bst = [2, 31, 5000, 5, 80000]
+    cst = [13, 1, 53, 3, 800]
+    A = g.standard_normal(300000)
+    B = g.standard_normal(300000)
+    Cm = g.standard_normal(4000)
+    ref = ref_gemm_vec(m, n, k, batch, m0, n0, k0e, A, ast, B, bst, Cm, cst, 1.25, 0.0)
+    got = Cm.copy()
+    a_s, ap = lptr(ast)
+    b_s, bp = lptr(bst)
+    c_s, cp = lptr(cst)
+    ks = C.c_int(0)
+    ctx.check(lib.ttc_test_gemm_runs(ctx.h, m, n, k, batch, m0, n0, k0e, ptr(A), A.size, ap, ptr(B), B.size, bp,
+                                     ptr(got), got.size, cp, 1.25, 0.0, 2, C.byref(ks)))
+    assert ks.value > 1
+    assert np.allclose(got, ref, rtol=1e-12, atol=1e-11)
+
+
 @pytest.mark.parametrize("m,n", [(1, 1), (7, 3), (3, 7), (64, 64), (100, 37), (512, 256), (300, 300), (768, 384),
                                  (700, 690), (1044, 522)])
 def test_householder_qr(ctx, m, n):
