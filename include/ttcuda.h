@@ -232,6 +232,14 @@ int ttc_ttrand_rounding_op(ttc_context* ctx, int32_t m, const double* alpha, con
 int ttc_ttrand_rounding_residual(ttc_context* ctx, const ttc_tto* A, const ttc_ttv* x, const ttc_ttv* b,
                                  const int64_t* rks, const ttc_sketch_opts* sk, ttc_ttv_out* y);
 
+/* stta(alpha, ys, rks; seed_left, seed_right, orthogonal, block_rks), src/tt_randtools.jl:551-641
+ * (m == 1, alpha[0] == 1: stta(y, rks; ...)): streaming TT approximation of sum_j alpha_j ys[j]
+ * from a forward sketch (block counts oversampled 1.5x, src/sketches.jl:1126-1160) and a reverse
+ * one.  rks: N+1 target ranks, boundary ranks 1.  Output rank k is the smaller of the two sketch
+ * ranks of bond k; ot = 0. */
+int ttc_stta(ttc_context* ctx, int32_t m, const double* alpha, const ttc_ttv* ys, const int64_t* rks,
+             uint64_t seed_left, uint64_t seed_right, int32_t orthogonal, int64_t block_rks, ttc_ttv_out* y);
+
 /* *(A::TToperator, v::TTvector), src/tt_operations.jl:170-194.  Output ranks
  * R_k * r_k with the operator index fastest; ot = 0. */
 int ttc_mpo_apply(ttc_context* ctx, const ttc_tto* A, const ttc_ttv* x, ttc_ttv_out* y);

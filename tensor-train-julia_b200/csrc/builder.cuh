@@ -47,6 +47,7 @@ struct Builder {
   // FP64 -> BF16, or FP64 -> FP32 rounded to TF32 (f32 = true)
   void cvt_bf16(const std::vector<CvtDesc>& v, bool f32 = false);
   void zerochk(const std::vector<ZeroChkDesc>& v);
+  void pinv_scale(const std::vector<PinvScaleDesc>& v);
   void finalize(const std::vector<FinalDesc>& v);
   void setrank(const std::vector<SetRankDesc>& v);
 };

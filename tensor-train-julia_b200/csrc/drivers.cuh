@@ -24,6 +24,11 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
                    double tol, long long rmax);
 void emit_zero_check(Builder& B, ttc_batch* y, const std::vector<int>& tts, int core, double tol);
 void emit_finalize(Builder& B, ttc_batch* y, const std::vector<int>& tts, const std::vector<std::vector<int>>& rp);
+// Shape of the sketch blocks of one site: p blocks of (left, n, right) in the Julia layout.
+struct BlockShape {
+  int left, n, right, p;
+};
+void emit_block_draws(Builder& B, const std::vector<BlockShape>& sh, const ttc_sketch_opts& o, std::vector<double*>& raw);
 void emit_sketch_blocks(Builder& B, const std::vector<long long>& dims, const SketchPlan& sp, const ttc_sketch_opts& o,
                         const std::vector<const double*>& host_raw, std::vector<double*>& S);
 void emit_sketch_f64(Builder& B, ttc_batch* x, const std::vector<int>& tts, const SketchPlan& sp,

@@ -304,22 +304,20 @@ SketchPlan sketch_plan(const std::vector<long long>& dims, const std::vector<lon
   return sp;
 }
 
-// Emit generation of the raw sketch blocks (Julia layout (b_{k+1}, n, b_k, p_k)) into raw[k]
-// and their permutation into the GEMM layout (n, b_{k+1}, b_k, p_k) in S[k].
-void emit_sketch_blocks(Builder& B, const std::vector<long long>& dims, const SketchPlan& sp, const ttc_sketch_opts& o,
-                        const std::vector<const double*>& host_raw, std::vector<double*>& S) {
-  const int N = (int)dims.size();
-  S.assign(N, nullptr);
-  std::vector<double*> raw(N, nullptr);
+// Emit the draws of sketch blocks (src/sketches.jl:44-84): for site k, p blocks of shape
+// (left, n, right) in the Julia layout, from the Philox stream (seed, k); orthogonal blocks are
+// the Q factors of the (left n x right) Gaussian blocks scaled by sqrt(left n / right), or the
+// identity when right == left n; Gaussian blocks are scaled by 1/sqrt(right).
+void emit_block_draws(Builder& B, const std::vector<BlockShape>& sh, const ttc_sketch_opts& o, std::vector<double*>& raw) {
+  const int N = (int)sh.size();
+  raw.assign(N, nullptr);
   std::vector<PhiloxDesc> ph;
   std::vector<QRDesc> qr;
-  std::vector<CopyDesc> cpQ, cpS;
+  std::vector<CopyDesc> cpQ;
   std::vector<ZeroDesc> zr;
   for (int k = 0; k < N; ++k) {
-    const long long bl = sp.b[k + 1], n = dims[k], br = sp.b[k], pk = sp.p[k];
+    const long long bl = sh[k].left, n = sh[k].n, br = sh[k].right, pk = sh[k].p;
     const long long cnt = bl * n * br * pk;
-    S[k] = B.wd(cnt);
-    if (!host_raw.empty()) { raw[k] = const_cast<double*>(host_raw[k]); continue; }
     raw[k] = B.wd(cnt);
     const bool orth = o.orthogonal != 0;
     const bool ident = orth && (br == bl * n);
@@ -352,6 +350,25 @@ void emit_sketch_blocks(Builder& B, const std::vector<long long>& dims, const Sk
   B.zero(zr);
   B.qr(qr);
   B.copy(cpQ);
+}
+
+// Emit generation of the raw sketch blocks of the reverse sketch (Julia layout
+// (b_{k+1}, n, b_k, p_k)) into raw[k] and their permutation into the GEMM layout
+// (n, b_{k+1}, b_k, p_k) in S[k].
+void emit_sketch_blocks(Builder& B, const std::vector<long long>& dims, const SketchPlan& sp, const ttc_sketch_opts& o,
+                        const std::vector<const double*>& host_raw, std::vector<double*>& S) {
+  const int N = (int)dims.size();
+  S.assign(N, nullptr);
+  std::vector<double*> raw(N, nullptr);
+  std::vector<CopyDesc> cpS;
+  for (int k = 0; k < N; ++k) S[k] = B.wd((size_t)sp.b[k + 1] * dims[k] * sp.b[k] * sp.p[k]);
+  if (!host_raw.empty()) {
+    for (int k = 0; k < N; ++k) raw[k] = const_cast<double*>(host_raw[k]);
+  } else {
+    std::vector<BlockShape> sh(N);
+    for (int k = 0; k < N; ++k) sh[k] = {sp.b[k + 1], (int)dims[k], sp.b[k], sp.p[k]};
+    emit_block_draws(B, sh, o, raw);
+  }
   for (int k = 0; k < N; ++k) {
     const long long bl = sp.b[k + 1], n = dims[k], br = sp.b[k], pk = sp.p[k];
     // raw (be, z, b, j) at be + bl*(z + n*(b + br*j))  ->  S (z, be, (b, j)) at z + n*be + n*bl*(b + br*j)

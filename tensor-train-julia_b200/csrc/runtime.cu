@@ -21,6 +21,31 @@ void launch_zerochk(const ZeroChkDesc* d, int count, cudaStream_t s) {
   TTC_CHECK_LAUNCH();
 }
 
+// One CTA per problem: the largest sigma (block reduction), then the column scaling.
+__global__ void pinv_scale_kernel(const PinvScaleDesc* descs) {
+  const PinvScaleDesc D = descs[blockIdx.x];
+  __shared__ double s_max[32];
+  double mx = 0.0;
+  for (int i = threadIdx.x; i < D.n; i += blockDim.x) mx = fmax(mx, D.sigma[i]);
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  mx = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mx = fmax(mx, s_max[w]);
+  const double thr = D.eps * mx;
+  for (long long e = threadIdx.x; e < (long long)D.m * D.n; e += blockDim.x) {
+    const int i = (int)(e / D.m), r = (int)(e - (long long)i * D.m);
+    const double s = D.sigma[i];
+    double* x = D.X + (long long)i * D.ldx + r;
+    *x = (s > thr) ? *x / (s * s) : 0.0;
+  }
+}
+void launch_pinv_scale(const PinvScaleDesc* d, int count, cudaStream_t s) {
+  if (count <= 0) return;
+  pinv_scale_kernel<<<count, 256, 0, s>>>(d);
+  TTC_CHECK_LAUNCH();
+}
+
 __global__ void final_kernel(const FinalDesc* descs) {
   const FinalDesc D = descs[blockIdx.y];
   if (*D.flag == 0) return;
@@ -136,6 +161,7 @@ static void launch_op(ttc_context* c, const Plan& p, const Op& op) {
       case OP_PHILOX: launch_philox((const PhiloxDesc*)d, op.count, op.total, s); break;
       case OP_BF16GEMM: launch_gemm_bf16_tc((const Bf16GemmDesc*)d, op.count, op.total, s, c->d_flags, op.a != 0); break;
       case OP_ZEROCHK: launch_zerochk((const ZeroChkDesc*)d, op.count, s); break;
+      case OP_PINV_SCALE: launch_pinv_scale((const PinvScaleDesc*)d, op.count, s); break;
       case OP_FINAL: launch_final((const FinalDesc*)d, op.count, op.total, s); break;
       case OP_SETRANK: launch_setrank((const SetRankDesc*)d, op.count, s); break;
       case OP_CVT_BF16: launch_cvt_bf16((const CvtDesc*)d, op.count, op.total, s, op.a != 0); break;
@@ -647,6 +673,15 @@ void Builder::cvt_bf16(const std::vector<CvtDesc>& v, bool f32) {
     }
   }
   Op op; op.kind = OP_CVT_BF16; op.off = plan->push(v); op.count = (int)v.size(); op.total = mx; op.a = f32;
+  plan->ops.push_back(op);
+}
+void Builder::pinv_scale(const std::vector<PinvScaleDesc>& v) {
+  if (v.empty()) return;
+  for (auto& d : v) {
+    chk(wsbase != nullptr, d.X, (long long)d.ldx * std::max(d.n - 1, 0) + d.m, 8, "pinv_scale X");
+    chk(wsbase != nullptr, d.sigma, d.n, 8, "pinv_scale sigma");
+  }
+  Op op; op.kind = OP_PINV_SCALE; op.off = plan->push(v); op.count = (int)v.size();
   plan->ops.push_back(op);
 }
 void Builder::zerochk(const std::vector<ZeroChkDesc>& v) {

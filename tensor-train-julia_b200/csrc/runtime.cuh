@@ -23,7 +23,7 @@ constexpr int kEvRunBegin = 6, kEvRunEnd = 7;
 enum OpKind {
   OP_GEMM, OP_QR, OP_JACOBI, OP_TRUNC, OP_SELECT, OP_COPY, OP_ZERO, OP_SUMSQ, OP_APPLY,
   OP_PHILOX, OP_BF16GEMM, OP_ZEROCHK, OP_FINAL, OP_STAGE, OP_CVT_BF16, OP_SETRANK, OP_QAPPLY, OP_GEMM32, OP_CVT32,
-  OP_WIDEN
+  OP_WIDEN, OP_PINV_SCALE
 };
 
 struct Op {
@@ -51,6 +51,11 @@ struct SetRankDesc { int* dst; const int* src; int n; };
 // FP64 -> BF16 conversion with a 2-level index map: dst[i*ds_i + j*ds_j] = bf16(src[i*ss_i + j*ss_j]).
 struct CvtDesc { const double* src; void* dst; long long rows, cols, ss_i, ss_j, ds_i, ds_j; double alpha; };
 
+// Column scaling of a pseudo-inverse from a one-sided Jacobi SVD: X (m x n, ldx) holds A V
+// (orthogonal columns, norms sigma); column i becomes X[:, i] / sigma_i^2 when
+// sigma_i > eps * max(sigma), else zero (the kept set of src/tt_randtools.jl:485-489).
+struct PinvScaleDesc { double* X; int ldx; int m, n; const double* sigma; double eps; };
+void launch_pinv_scale(const PinvScaleDesc* d, int count, cudaStream_t s);
 void launch_zerochk(const ZeroChkDesc* d, int count, cudaStream_t s);
 void launch_final(const FinalDesc* d, int count, long long max_n, cudaStream_t s);
 void launch_setrank(const SetRankDesc* d, int count, cudaStream_t s);

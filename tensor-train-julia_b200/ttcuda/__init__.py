@@ -479,6 +479,50 @@ def ttrand_rounding_residual(A: TToperator, y: TTvector, b: TTvector, rks=None, 
     return out.tt()
 
 
+def _fwd_sketch_ranks(dims, rks, block_rks, oversampling=1.5):
+    """Sketch ranks b .* p of the forward sketch (src/sketches.jl:243-258) with block-count oversampling."""
+    N = len(dims)
+    b = [1] + [block_rks if block_rks else N] * N
+    for k in range(N):
+        b[k + 1] = min(b[k + 1], dims[k] * b[k])
+    p = [int(math.ceil(r / bb)) for r, bb in zip(rks, b)]
+    for i in range(N - 1, 0, -1):
+        p[i] = max(p[i], p[i + 1])
+    p[0] = 1
+    if oversampling != 1:
+        p = [p[0]] + [int(math.ceil(oversampling * v)) for v in p[1:]]
+    return [bb * pp for bb, pp in zip(b, p)]
+
+
+def stta_lincomb(alpha: Sequence[float], ys: Sequence[TTvector], rks=None, seed_left=1234, seed_right=5678,
+                 orthogonal=True, block_rks=None) -> TTvector:
+    """stta(alpha, y, rks; seed_left, seed_right, orthogonal, block_rks), src/tt_randtools.jl:592-641:
+    streaming TT approximation of sum_j alpha_j ys[j] from two-sided sketches."""
+    if len(alpha) != len(ys):
+        raise DimensionMismatch("stta: length(alpha) != length(y)")
+    N = ys[0].N
+    rks = _rks_arg(rks, N, lambda: default_rank_heuristic(list(ys)))
+    sl = _fwd_sketch_ranks(ys[0].ttv_dims, rks, block_rks)
+    sr = _sketch_ranks(ys[0].ttv_dims, rks, block_rks)
+    caps = [1] + [min(a, b) for a, b in zip(sl[1:N], sr[1:N])] + [1]
+    ctx = get_context()
+    keep = _Keep()
+    arr = (L.TTV * len(ys))(*[_ttv(t, keep) for t in ys])
+    al = np.ascontiguousarray(alpha, dtype=np.float64)
+    out = _Out(ys[0].ttv_dims, caps)
+    ctx.check(lib.ttc_stta(ctx.h, len(ys), al.ctypes.data_as(L.P_f64), arr, _i64(rks, keep),
+                           int(seed_left) & 0xFFFFFFFFFFFFFFFF, int(seed_right) & 0xFFFFFFFFFFFFFFFF,
+                           1 if orthogonal else 0, int(block_rks or 0), C.byref(out.s)))
+    return out.tt()
+
+
+def stta(y: TTvector, rks=None, seed_left=1234, seed_right=5678, orthogonal=True, block_rks=None) -> TTvector:
+    """stta(y, rks; seed_left, seed_right, orthogonal, block_rks), src/tt_randtools.jl:551-590 (rks
+    vector, int rmax, or the default heuristic)."""
+    rks = _rks_arg(rks, y.N, lambda: default_rank_heuristic(y))
+    return stta_lincomb([1.0], [y], rks, seed_left, seed_right, orthogonal, block_rks)
+
+
 def mpo_apply(A: TToperator, v: TTvector) -> TTvector:
     """*(A::TToperator, v::TTvector), src/tt_operations.jl:170-194."""
     if tuple(A.tto_dims) != tuple(v.ttv_dims):
