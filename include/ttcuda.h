@@ -232,6 +232,14 @@ int ttc_ttrand_rounding_op(ttc_context* ctx, int32_t m, const double* alpha, con
 int ttc_ttrand_rounding_residual(ttc_context* ctx, const ttc_tto* A, const ttc_ttv* x, const ttc_ttv* b,
                                  const int64_t* rks, const ttc_sketch_opts* sk, ttc_ttv_out* y);
 
+/* ttrand_rounding(y::NTuple{M,TTvector}, rks; orthogonal, seed, block_rks), src/tt_randtools.jl:364-473:
+ * randomized rounding of the Hadamard product ys[0] .* ... .* ys[m-1] (m == 1: ttrand_rounding
+ * of ys[0]).  The last factor is never multiplied out: its sketch and projection contractions are
+ * the structured (Kronecker) ones of src/sketches.jl:1735-1881; the first m-1 are multiplied out
+ * on the device.  FP64 sketch only.  Output ranks as ttc_ttrand_rounding. */
+int ttc_ttrand_rounding_hadamard(ttc_context* ctx, int32_t m, const ttc_ttv* ys, const int64_t* rks,
+                                 const ttc_sketch_opts* sk, ttc_ttv_out* y);
+
 /* stta(alpha, ys, rks; seed_left, seed_right, orthogonal, block_rks), src/tt_randtools.jl:551-641
  * (m == 1, alpha[0] == 1: stta(y, rks; ...)): streaming TT approximation of sum_j alpha_j ys[j]
  * from a forward sketch (block counts oversampled 1.5x, src/sketches.jl:1126-1160) and a reverse

@@ -78,6 +78,8 @@ void recursive_sketch_host(ttc_context* c, const ttc_ttv* A, const ttc_tto* H, c
 void rand_rounding_host(ttc_context* c, int m, const double* alpha, const ttc_tto* A, const ttc_ttv* ys,
                         const ttc_round_opts* after, const int64_t* rks, const ttc_sketch_opts& sk, ttc_ttv_out* y);
 void mpo_apply_host(ttc_context* c, const ttc_tto* A, const ttc_ttv* x, ttc_ttv_out* y);
+void hadamard_rounding_host(ttc_context* c, int m, const ttc_ttv* ys, const int64_t* rks, const ttc_sketch_opts& sk,
+                            ttc_ttv_out* y);
 void stta_host(ttc_context* c, int m, const double* alpha, const ttc_ttv* ys, const int64_t* rks, uint64_t seed_left,
                uint64_t seed_right, int orthogonal, int64_t block_rks, ttc_ttv_out* y);
 double dot_host(ttc_context* c, const ttc_ttv* A, const ttc_ttv* B, double* const* W_out, int reverse);

@@ -689,6 +689,19 @@ int ttc_ttrand_rounding_lincomb(ttc_context* c, int32_t m, const double* alpha, 
   return guard(c, [&] { rand_rounding_host(c, m, alpha, nullptr, ys, nullptr, rks, *sk, y); });
 }
 
+int ttc_ttrand_rounding_hadamard(ttc_context* c, int32_t m, const ttc_ttv* ys, const int64_t* rks,
+                                 const ttc_sketch_opts* sk, ttc_ttv_out* y) {
+  if (!c || m < 1 || !ys || !rks || !sk || !y) return TTC_EARG;
+  return guard(c, [&] {
+    if (m == 1) {
+      const double one = 1.0;
+      rand_rounding_host(c, 1, &one, nullptr, ys, nullptr, rks, *sk, y);
+    } else {
+      hadamard_rounding_host(c, m, ys, rks, *sk, y);
+    }
+  });
+}
+
 int ttc_stta(ttc_context* c, int32_t m, const double* alpha, const ttc_ttv* ys, const int64_t* rks, uint64_t seed_left,
              uint64_t seed_right, int32_t orthogonal, int64_t block_rks, ttc_ttv_out* y) {
   if (!c || m < 1 || !alpha || !ys || !rks || !y) return TTC_EARG;

@@ -479,6 +479,25 @@ def ttrand_rounding_residual(A: TToperator, y: TTvector, b: TTvector, rks=None, 
     return out.tt()
 
 
+def ttrand_rounding_hadamard(ys: Sequence[TTvector], rks, orthogonal=True, seed=1234, block_rks=None,
+                             sketch_blocks=None) -> TTvector:
+    """ttrand_rounding(y::NTuple, rks; ...) (src/tt_randtools.jl:364-473): randomized rounding of
+    the Hadamard product ys[0] .* ys[1] .* ... without forming it for the last factor.  rks: a
+    vector or an int rmax (the reference's default heuristic has no method for tuples)."""
+    N = ys[0].N
+    if rks is None:
+        raise ArgumentError("ttrand_rounding of a Hadamard product needs rks (a vector or an int rmax)")
+    rks = _rks_arg(rks, N, None)
+    s = _sketch_ranks(ys[0].ttv_dims, rks, block_rks)
+    ctx = get_context()
+    keep = _Keep()
+    arr = (L.TTV * len(ys))(*[_ttv(t, keep) for t in ys])
+    so = _sketch_opts(orthogonal, seed, block_rks, "fp64", sketch_blocks, keep)
+    out = _Out(ys[0].ttv_dims, _rand_out_caps(ys[0].ttv_dims, s))
+    ctx.check(lib.ttc_ttrand_rounding_hadamard(ctx.h, len(ys), arr, _i64(rks, keep), C.byref(so), C.byref(out.s)))
+    return out.tt()
+
+
 def _fwd_sketch_ranks(dims, rks, block_rks, oversampling=1.5):
     """Sketch ranks b .* p of the forward sketch (src/sketches.jl:243-258) with block-count oversampling."""
     N = len(dims)

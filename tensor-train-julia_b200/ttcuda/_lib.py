@@ -83,6 +83,7 @@ _SIGS = {
     "ttc_recursive_sketch_op": (i32, [vp, C.POINTER(TTO), C.POINTER(TTV), P_i64, C.POINTER(SketchOpts), PP_f64, P_i64]),
     "ttc_ttrand_rounding": (i32, [vp, C.POINTER(TTV), P_i64, C.POINTER(SketchOpts), C.POINTER(TTVOut)]),
     "ttc_ttrand_rounding_lincomb": (i32, [vp, i32, P_f64, C.POINTER(TTV), P_i64, C.POINTER(SketchOpts), C.POINTER(TTVOut)]),
+    "ttc_ttrand_rounding_hadamard": (i32, [vp, i32, C.POINTER(TTV), P_i64, C.POINTER(SketchOpts), C.POINTER(TTVOut)]),
     "ttc_stta": (i32, [vp, i32, P_f64, C.POINTER(TTV), P_i64, C.c_uint64, C.c_uint64, i32, C.c_int64,
                        C.POINTER(TTVOut)]),
     "ttc_ttrand_rounding_op": (i32, [vp, i32, P_f64, C.POINTER(TTO), C.POINTER(TTV), P_i64, C.POINTER(SketchOpts),
