@@ -393,6 +393,68 @@ def other_configs(ttcuda, ctx, hbm_peak, stream):
         "gemm_f64": {"ms": gf5[0], "launches": gf5[1], "tflop": gf5[2] / 1e12,
                      "tflops": (gf5[2] / (gf5[0] / 1e3) / 1e12) if gf5[0] > 0 else None},
         "profile_ms": {k: round(v[0], 3) for k, v in prof5.items() if v[1]}}
+    out["callers"] = callers(ttcuda, ctx, stream, H, dims2)
+    return out
+
+
+def callers(ttcuda, ctx, stream, H, dims2):
+    """The rounding path's callers on config-2/config-3 sizes: sketched Rayleigh-Ritz on the
+    16-site Hubbard MPO, STTA of a rank-128 TT, and the randomized rounding of a Hadamard product
+    (structured, against multiplying the product out and rounding it), each through the public
+    API on host tensors."""
+    import ttcuda.solvers as ts
+    out = {}
+    g = np.random.default_rng(60)
+    # sketched Rayleigh-Ritz: 10 Krylov vectors, rmax 32, from a rank-16 start, on the MPO scaled by
+    # 1/20 (the solver's tol = res_sketch^2 / 2 is a relative tolerance, so the operator's scale
+    # must keep the sketched residual below 1)
+    Hs = ttcuda.TToperator(32, [H.tto_vec[0] * 0.05] + list(H.tto_vec[1:]), H.tto_dims, H.tto_rks)
+    r16 = r_and_d([1] + [16] * 31 + [1], dims2, 16)
+    b0 = ttcuda.TTvector(32, rand_cores(dims2, r16, g, normalise=True), dims2, r16)
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    e, psi, hist = ts.sketched_rayleigh_ritz(Hs, b0, 10, 32)
+    ctx.synchronize()
+    t_rr = time.perf_counter() - t0
+    out["sketched_rayleigh_ritz"] = {
+        "workload": "sketched_rayleigh_ritz(H/20, b0, d=10, rmax=32): H the 16-site Hubbard MPO (t=1, U=4), b0 rank 16",
+        "value": 10 / t_rr, "unit": "Krylov steps/s (wall clock, host linear algebra and transfers included)",
+        "s": t_rr, "e_sketch": e, "e_true": hist[-1]["e_true"], "res_sketch": hist[-1]["res_sketch"],
+        "e_true_history": [h["e_true"] for h in hist]}
+    # STTA of a rank-128 TT (d=32, n=2, bond singular values 10^(-i/32)) to rank 64, against the
+    # deterministic rounding to rank 64
+    r128 = r_and_d([1] + [128] * 31 + [1], dims2, 128)
+    x = ttcuda.TTvector(32, make_tt(dims2, r128, 61), dims2, r128)
+    ms_st = device_ms(ctx, lambda: ttcuda.stta(x, 64, block_rks=8), 3, stream)
+    ms_tr = device_ms(ctx, lambda: ttcuda.tt_rounding(x, rmax=64), 3, stream)
+    zs, zt = ttcuda.stta(x, 64, block_rks=8), ttcuda.tt_rounding(x, rmax=64)
+
+    def rel(a, b):
+        return ttcuda.norm(ttcuda.tt_add(a, ttcuda.tt_scale(-1.0, b))) / ttcuda.norm(b)
+    out["stta"] = {"workload": "stta(x, 64; block_rks=8), x rank 128, d=32, n=2, bond singular values 10^(-i/32)",
+                   "value": 1e3 / ms_st, "unit": "approximations/s", "ms": ms_st,
+                   "path": "ttc_stta on host tensors", "rel_err": rel(zs, x),
+                   "tt_rounding_rmax64": {"ms": ms_tr, "rel_err": rel(zt, x)}}
+    # Hadamard product of two rank-32 TTs (product rank 1024), rounded with sketch rank 64
+    r32 = r_and_d([1] + [32] * 31 + [1], dims2, 32)
+    x1 = ttcuda.TTvector(32, rand_cores(dims2, r32, g, normalise=True), dims2, r32)
+    x2 = ttcuda.TTvector(32, rand_cores(dims2, r32, g, normalise=True), dims2, r32)
+    ms_h = device_ms(ctx, lambda: ttcuda.ttrand_rounding_hadamard([x1, x2], 64), 3, stream)
+    zh = ttcuda.ttrand_rounding_hadamard([x1, x2], 64)
+    # the product multiplied out on the host (slice-wise Kronecker cores) and rounded on the GPU
+    vec = []
+    for k in range(32):
+        a, b = x1.ttv_vec[k], x2.ttv_vec[k]
+        vec.append(np.asfortranarray(np.stack([np.kron(a[i], b[i]) for i in range(2)])))
+    rp = [p * q for p, q in zip(x1.ttv_rks, x2.ttv_rks)]
+    P = ttcuda.TTvector(32, vec, dims2, rp)
+    ms_p = device_ms(ctx, lambda: ttcuda.ttrand_rounding(P, 64), 3, stream)
+    zp = ttcuda.ttrand_rounding(P, 64)
+    out["hadamard_rounding"] = {
+        "workload": "ttrand_rounding((x1, x2), 64): x1, x2 rank 32, d=32, n=2 (product rank 1024)",
+        "value": 1e3 / ms_h, "unit": "roundings/s", "ms": ms_h, "path": "ttc_ttrand_rounding_hadamard on host tensors",
+        "formed_product": {"ms": ms_p, "path": "ttc_ttrand_rounding of the product multiplied out on the host (rank-1024 cores, 512 MB uploaded per call)"},
+        "rel_diff_vs_formed": rel(zh, zp)}
     return out
 
 
@@ -429,6 +491,41 @@ def kernel_bench(reps):
                       "results": out}), flush=True)
 
 
+def jacobi_bench(reps, count=64, n=256):
+    """The batched one-sided Jacobi SVD alone on `count` QR-LQ preconditioned n x n factors whose
+    singular values decay as 10^(-i/32) (the SVD-sweep problems of the headline workload at full
+    rank), CUDA events around `reps` launches (each after a copy of the inputs); prints one JSON
+    line with the sweep counts and the work rate (6 m n^2 flops per sweep: the dot products and
+    rotations of all n (n - 1) / 2 column pairs)."""
+    import ctypes as C
+    import torch  # noqa: F401
+    import ttcuda
+    from ttcuda._lib import lib
+    lib.ttc_test_jacobi_bench.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_int,
+                                          C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    lib.ttc_test_jacobi_bench.restype = C.c_int
+    ctx = ttcuda.Context(0)
+    g = np.random.default_rng(7)
+    mats = []
+    sig = 10.0 ** (-np.arange(n) / 32.0)
+    for _ in range(count):
+        u, _ = np.linalg.qr(g.standard_normal((n, n)))
+        v, _ = np.linalg.qr(g.standard_normal((n, n)))
+        a = (u * sig) @ v.T
+        _, r1 = np.linalg.qr(a.T)                 # M^T = Q R1, then R1^T = Q2 R2: Jacobi on R2^T
+        _, r2 = np.linalg.qr(r1.T)
+        mats.append(np.asfortranarray(r2.T))
+    X = np.concatenate([m.ravel(order="F") for m in mats])
+    ms = C.c_double()
+    sw = np.zeros(count, dtype=np.int32)
+    ctx.check(lib.ttc_test_jacobi_bench(ctx.h, count, n, n, X.ctypes.data_as(C.POINTER(C.c_double)), reps,
+                                        C.byref(ms), sw.ctypes.data_as(C.POINTER(C.c_int))))
+    work = float(np.abs(sw).sum()) * 6.0 * n * n * n     # per sweep: n^2 / 2 pairs of 12 m flops
+    print(json.dumps({"jacobi_bench": "jacobi_svd_kernel", "count": count, "m": n, "n": n, "ms": ms.value,
+                      "sweeps_mean": float(np.abs(sw).mean()), "sweeps_max": int(np.abs(sw).max()),
+                      "work_tflops": work / (ms.value / 1e3) / 1e12}), flush=True)
+
+
 # ---------------------------------------------------------------------------- ours
 def main():
     ap = argparse.ArgumentParser()
@@ -438,6 +535,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--jacobi-bench", action="store_true",
+                    help="time the batched Jacobi SVD alone on 64 preconditioned 256 x 256 factors")
     ap.add_argument("--no-other-configs", action="store_true", help="skip the config 1, 2, 4 and 5 lines")
     ap.add_argument("--kernel-bench", action="store_true",
                     help="time the tcgen05 sketch GEMM alone on the config-5 shapes and exit")
@@ -451,6 +550,9 @@ def main():
         return
     if args.kernel_bench:
         kernel_bench(max(3, args.steps))
+        return
+    if args.jacobi_bench:
+        jacobi_bench(max(1, args.steps))
         return
 
     import torch

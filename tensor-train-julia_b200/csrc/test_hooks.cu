@@ -204,6 +204,42 @@ int ttc_test_jacobi(ttc_context* c, int m, int n, double* X, int accw, double* W
   });
 }
 
+// The batched Jacobi SVD alone: `count` m x n problems (X, column-major, one after another) are
+// copied into a work array and factored, `reps` times in one plan run; *ms receives the device time
+// per repetition (copy included) and sweeps[i] the sweeps problem i used in the last repetition.
+int ttc_test_jacobi_bench(ttc_context* c, int count, int m, int n, const double* X, int reps, double* ms,
+                          int* sweeps) {
+  return hook(c, [&] {
+    TTC_REQUIRE(count >= 1 && m >= n && n >= 1 && reps >= 1, TTC_EARG, "jacobi bench: bad sizes");
+    const size_t per = (size_t)m * n;
+    DevBuf d0(per * count * 8), dX(per * count * 8), ds((size_t)n * count * 8), dp((size_t)n * count * 4),
+        di((size_t)count * 4);
+    TTC_CUDA(cudaMemcpy(d0.p, X, per * count * 8, cudaMemcpyHostToDevice));
+    static unsigned long long serial = 0;
+    const std::string key = "hook-jacobi:" + std::to_string(++serial);
+    Plan* p = get_plan(c, key, [&](Builder& B) {
+      for (int r = 0; r < reps; ++r) {
+        if (r == 0) B.stage(0);
+        B.copy({cd2(d0.as<double>(), dX.as<double>(), (long long)(per * count), 1, 1, 0, 1, 0)});
+        std::vector<JacobiDesc> v;
+        for (int i = 0; i < count; ++i)
+          v.push_back({m, n, dX.as<double>() + per * i, m, nullptr, n, ds.as<double>() + (size_t)n * i,
+                       dp.as<int>() + (size_t)n * i, di.as<int>() + i, nullptr, 0});
+        B.jacobi(v);
+      }
+      B.stage(1);
+    });
+    run_plan(c, *p);
+    TTC_CUDA(cudaStreamSynchronize(c->stream));
+    float t = 0.f;
+    TTC_CUDA(cudaEventElapsedTime(&t, c->ev[0], c->ev[1]));
+    *ms = (double)t / reps;
+    TTC_CUDA(cudaMemcpy(sweeps, di.p, (size_t)count * 4, cudaMemcpyDeviceToHost));
+    c->plans.erase(key);
+    TTC_CUDA(cudaMemset(c->d_flags, 0, sizeof(int)));
+  });
+}
+
 // tcgen05 BF16 GEMM: C (m x n, col-major, FP64 out) = alpha * bf16(A) bf16(B)^T with A (m x k)
 // and B (n x k) given row-major in FP64 (converted to BF16 on the device).
 int ttc_test_bf16_gemm(ttc_context* c, int m, int n, int k, const double* A, const double* Bh, double* C,
