@@ -104,6 +104,20 @@ def heuristic(rank_lists):
     return rks
 
 
+def compressing_levels(dims, rank_lists, s):
+    """(TT, bond) pairs whose range finder compresses: the sketch rank s_{k+1} is below both
+    dimensions of y_k's unfolding (n_k e_k x r_{k+1}, e the sweep's effective ranks).  Only these
+    read the sketch when the SVD sweep follows; with none, the library skips the sketch."""
+    count = 0
+    for r in rank_lists:
+        e = 1
+        for k in range(len(dims) - 1):
+            q = min(dims[k] * e, r[k + 1], s[k + 1])
+            count += q == s[k + 1]
+            e = q
+    return count
+
+
 # ------------------------------------------------------------------------ clocks
 class ClockSampler:
     def __init__(self, path):
@@ -582,6 +596,7 @@ def main():
     block = D                        # ttrand_rounding's default block_rks = N
     s = ttcuda._sketch_ranks(dims, rks, block)
     rho = ttcuda._rand_out_caps(dims, s)
+    n_compress = compressing_levels(dims, ranks, s)
     xb = ttcuda.DeviceBatch.from_tts(tt_objs, ctx=ctx)
     y_mixed = ttcuda.DeviceBatch(dims, [rho] * len(tts), ctx=ctx)
     y_fp64 = ttcuda.DeviceBatch(dims, ranks, ctx=ctx)
@@ -652,6 +667,39 @@ def main():
     out_t = y_tf32.download()
     err_tf = max(rel_err(out_f[i], out_t[i]) for i in range(nerr))
     ranks_equal_tf = all(out_t[i].ttv_rks == out_f[i].ttv_rks for i in range(len(tts)))
+
+    # the same batch rounded to rank 64 (ttrand_rounding(y, 64) + SVD sweep, against tt_rounding with
+    # rmax = 64): here the sketch compresses every interior bond, the case randomized rounding is for
+    rmax_c = 64
+    rks_c = [1] + [rmax_c] * (D - 1) + [1]
+    s_c = ttcuda._sketch_ranks(dims, rks_c, block)
+    y_cm = ttcuda.DeviceBatch(dims, [ttcuda._rand_out_caps(dims, s_c)] * len(tts), ctx=ctx)
+    y_cf = ttcuda.DeviceBatch(dims, ranks, ctx=ctx)
+
+    def step_c_mixed(sync=False):
+        xb.round_rand(y_cm, rks_c, orthogonal=True, seed=1234, block_rks=block, precision="bf16",
+                      after_tol=TOL, rmax=rmax_c, sync=sync)
+
+    def step_c_fp64(sync=False):
+        xb.round_det(y_cf, tol=TOL, rmax=rmax_c, sync=sync)
+
+    for _ in range(max(3, args.warmup)):
+        step_c_mixed(sync=True)
+        step_c_fp64(sync=True)
+    ms_cm = timed(step_c_mixed, args.steps)
+    ms_cf = timed(step_c_fp64, args.steps)
+    out_cm, out_cf = y_cm.download(), y_cf.download()
+    compress_line = {
+        "variant": f"rank {rmax_c}: BF16-sketch ttrand_rounding(y, {rmax_c}) + FP64 SVD sweep (tol {TOL:g}, rmax "
+                   f"{rmax_c}) against deterministic tt_rounding(tol {TOL:g}, rmax {rmax_c})",
+        "mixed": {"value": shard.job_rate(job, args.steps, ms_cm), "ms_per_step": ms_cm / args.steps,
+                  "rel_err_max": max(rel_err(tt_objs[i], out_cm[i]) for i in range(nerr))},
+        "fp64": {"value": shard.job_rate(job, args.steps, ms_cf), "ms_per_step": ms_cf / args.steps,
+                 "rel_err_max": max(rel_err(tt_objs[i], out_cf[i]) for i in range(nerr))},
+        "mixed_over_fp64": ms_cf / ms_cm,
+        "range_finder_levels_compressing": compressing_levels(dims, ranks, s_c),
+        "unit": "roundings/s", "checked_tts": nerr,
+    }
 
     # per-kernel profile of one extra step of each variant (event pair around every launch)
     ctx.set_profiling(True)
@@ -762,6 +810,12 @@ def main():
                        "variant": "mixed: BF16-sketch (tcgen05) ttrand_rounding + FP64 SVD sweep",
                        "sketch_ranks": "default_rank_heuristic of the batch (r + ceil(max r/2)); block_rks = N, "
                                        "orthogonal blocks, seed 1234 (ttrand_rounding defaults)",
+                       "range_finder_levels_compressing": n_compress,
+                       "range_finder_levels": len(tts) * (D - 1),
+                       "range_finder_note": "a level compresses when its sketch rank is below both dimensions of "
+                                            "y_k's unfolding; with none, every range finder is a plain QR of y_k "
+                                            "and the library skips the sketch (the SVD sweep needs only range(Q)), "
+                                            "so the mixed and FP64 steps do the same FP64 work",
                        "l2": f"inputs {in_bytes / 1e6:.0f} MB resident > 126 MB L2"},
             "fp64": {"value": fp64_value, "unit": "roundings/s", "ms_per_step": ms_fp64 / args.steps,
                      "variant": "deterministic tt_rounding (FP64 Householder QR sweep + Jacobi SVD sweep)"},
@@ -772,6 +826,7 @@ def main():
                       "source": "torch.matmul 4096^3 FP64 and 8192^3 FP32 with TF32 allowed, best of 10, "
                                 "this run"},
             "mixed_over_fp64": value / fp64_value,
+            "rank_limited": compress_line,
             "accuracy": {"rel_err_mixed_max": err_mixed, "rel_err_fp64_max": err_fp64,
                          "rel_diff_mixed_vs_fp64": err_mf, "ranks_identical": ranks_equal,
                          "checked_tts": nerr},

@@ -44,11 +44,13 @@ inline void check_precision(int p) {
 }
 inline bool tensor_core_sketch(int p) { return p == TTC_PREC_BF16 || p == TTC_PREC_TF32; }
 // `complete`: write the completion columns of rank-deficient range finders (false when a truncated-SVD
-// sweep follows in the same plan); `eff` (optional) receives the effective ranks the cores are
-// nonzero within.
+// sweep follows in the same plan, which also selects the reduced forms that need only range(Q));
+// `eff` (optional) receives the effective ranks the cores are nonzero within.  W may hold null
+// pointers when `complete` is false and sketch_compresses() is false.
 void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<int>& tts, const SketchPlan& sp,
                      const std::vector<std::vector<double*>>& W, const std::vector<std::vector<int>>& rho,
                      bool complete = true, std::vector<std::vector<int>>* eff = nullptr);
+bool sketch_compresses(const ttc_batch* x, const std::vector<int>& tts, const SketchPlan& sp);
 std::vector<int> orth_left_ranks(const ttc_batch* x, int t);
 std::vector<int> rand_out_ranks(const std::vector<long long>& dims, const SketchPlan& sp);
 bool is_left_orth(const ttc_batch* x, int t);

@@ -444,6 +444,10 @@ void emit_sketch_f64(Builder& B, ttc_batch* x, const std::vector<int>& tts, cons
 // columns meet zero rows of y_{k+1}.  When the truncated-SVD sweep follows in the same plan
 // (`complete` false) the completion columns are not written: the sweep reads cores only up to
 // the effective ranks e, which `eff` returns, and the cores must stay zero beyond their ranks.
+// The sweep then also needs only range(Q), not the reference's basis of it, and the T and W
+// levels take their reduced forms: core k = Q1 with Q^T y_k = R1 (T), core k = I_m with
+// Q^T y_k = Y (W).  range(Q1 Q_M) = range(Q1) and range(Q_M) = R^m, so the represented tensor
+// and every singular value the SVD sweep sees are unchanged; the sketch is not read there.
 void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<int>& tts, const SketchPlan& sp,
                      const std::vector<std::vector<double*>>& W, const std::vector<std::vector<int>>& rho,
                      bool complete, std::vector<std::vector<int>>* eff) {
@@ -507,8 +511,10 @@ void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<i
       const double* Yk = (k == 0) ? x->core(t, 0) : Y[i];
       const long long yld = (k == 0) ? (long long)x->capr(t, 0) * n : m;
       const double* Wk = W[i][k + 1];                 // r_{k+1} x s, leading dimension r_{k+1}
-      double* P = B.wd((size_t)q * c);                 // Q^T y_k, its q nonzero rows
+      double* P = nullptr;                             // Q^T y_k, its q nonzero rows (leading dimension pld)
+      long long pld = q;
       if (q == s) {                                    // F
+        P = B.wd((size_t)q * c);
         double* Z = B.wd((size_t)m * s);
         double* Q = B.wd((size_t)m * s);
         double* Tws = B.wd(qr_tws(m, s));
@@ -516,12 +522,23 @@ void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<i
         qrZ.push_back({m, s, Z, m, Q, m, nullptr, 0, Tws});
         cpC.push_back(cd3(Q, core, e[i], n, s, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
         gp.push_back(gd(s, c, m, Q, m, 1, Yk, 1, yld, P, 1, s));
+      } else if (q == c && !complete) {                // T, reduced: core k = Q1, Q^T y_k = R1
+        double* Yw = const_cast<double*>(Yk);
+        if (k == 0) {
+          Yw = B.wd((size_t)m * c);
+          cp0.push_back(cd2(Yk, Yw, m, c, 1, yld, 1, m));
+        }
+        double* Q1 = B.wd((size_t)m * c);
+        P = B.wd((size_t)c * c);
+        qrY.push_back({m, c, Yw, m, Q1, m, P, c, B.wd(qr_tws(m, c))});
+        cpC.push_back(cd3(Q1, core, e[i], n, c, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
       } else if (q == c) {                             // T: c < m, c < s
         double* Yw = const_cast<double*>(Yk);
         if (k == 0) {                                  // the QR overwrites its input: not x's core
           Yw = B.wd((size_t)m * c);
           cp0.push_back(cd2(Yk, Yw, m, c, 1, yld, 1, m));
         }
+        P = B.wd((size_t)q * c);
         double* R1 = B.wd((size_t)c * c);
         double* M1 = B.wd((size_t)c * c);
         double* QM = B.wd((size_t)c * c);
@@ -545,7 +562,17 @@ void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<i
         cpC.push_back(cd3(Bq, core, e[i], n, ncols, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
         if (complete) outside_units(cpC, core, e[i], rh, n, yc, ncols, (long long)rhn - ncols);
         gp.push_back(gd(c, c, c, QM, c, 1, R1, 1, c, P, 1, c));
+      } else if (!complete) {                          // W, reduced: core k = I_m, Q^T y_k = Y
+        CopyDesc u{};
+        const long long cs = (long long)yc * n;        // column stride of the core's left unfolding
+        u.src = B.ctx->d_one; u.dst = core; u.alpha = 1.0;
+        u.ext[0] = e[i]; u.ext[1] = n; u.ext[2] = u.ext[3] = 1;
+        u.ds[0] = 1 + cs; u.ds[1] = yc + cs * e[i];    // row (a, z) -> column a + e z
+        cpC.push_back(u);
+        P = const_cast<double*>(Yk);
+        pld = yld;
       } else {                                         // W: q = m <= c, m < s
+        P = B.wd((size_t)q * c);
         double* M1 = B.wd((size_t)m * m);
         double* QM = B.wd((size_t)m * m);
         double* TwsM = B.wd(qr_tws(m, m));
@@ -556,7 +583,7 @@ void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<i
         gp.push_back(gd(m, c, m, QM, m, 1, Yk, 1, yld, P, 1, m));
       }
       // y_{k+1} = P A_{k+1}: (q, nn, r_{k+2}) compact
-      gy.push_back(gd(q, nn * r2, c, P, 1, q, x->core(t, k + 1), 1, x->capr(t, k + 1), Yn[i], 1, q));
+      gy.push_back(gd(q, nn * r2, c, P, 1, pld, x->core(t, k + 1), 1, x->capr(t, k + 1), Yn[i], 1, q));
       e[i] = q;
       if (eff) (*eff)[i][k + 1] = q;
     }
@@ -582,6 +609,23 @@ void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<i
   }
   B.copy(cp);
   B.release(mark0);
+}
+
+// Whether any level of emit_rand_sweep over the TTs `tts` of x takes the F form (q = s: the
+// sketch rank is below both of Y's dimensions, so the range finder compresses).  Follows the
+// sweep's effective ranks e on the host: e_0 = 1, e_{k+1} = min(n_k e_k, r_{k+1}, s_{k+1}).
+bool sketch_compresses(const ttc_batch* x, const std::vector<int>& tts, const SketchPlan& sp) {
+  const int N = x->N;
+  for (int t : tts) {
+    long long e = 1;
+    for (int k = 0; k + 1 < N; ++k) {
+      const long long m = x->dims[k] * e, c = x->rk(t, k + 1), s = sp.s[k + 1];
+      const long long q = std::min(std::min(m, c), s);
+      if (q == s) return true;
+      e = q;
+    }
+  }
+  return false;
 }
 
 std::vector<int> rand_out_ranks(const std::vector<long long>& dims, const SketchPlan& sp) {
@@ -623,15 +667,20 @@ void round_rand(ttc_context* c, ttc_batch* x, const std::vector<long long>& rks,
            (long long)o.block_rks, o.precision, after ? 1 : 0, after ? after->tol : 0.0, after ? (long long)after->rmax : 0LL);
   std::string key = std::string(kb) + raw_key + batch_key(x) + batch_out_key(y);
   for (long long r : rks) key += std::to_string(r) + ",";
+  // With the SVD sweep following, only F levels read the sketch (the reduced T and W forms of
+  // emit_rand_sweep do not): without one, the sketch is not computed.
+  const bool need_sketch = !after || sketch_compresses(x, all, sp);
   Plan* p = get_plan(c, key, [&](Builder& B) {
     B.stage(0);
     emit_zero_tts(B, y, all);
     emit_set_ranks(B, y, all, rho_all);
-    std::vector<double*> S;
-    emit_sketch_blocks(B, x->dims, sp, o, host_raw, S);
-    std::vector<std::vector<double*>> W;
-    if (tensor_core_sketch(o.precision)) emit_sketch_bf16(B, x, all, sp, S, W, o.precision == TTC_PREC_TF32);
-    else emit_sketch_f64(B, x, all, sp, S, W);
+    std::vector<std::vector<double*>> W(all.size(), std::vector<double*>(N + 1, nullptr));
+    if (need_sketch) {
+      std::vector<double*> S;
+      emit_sketch_blocks(B, x->dims, sp, o, host_raw, S);
+      if (tensor_core_sketch(o.precision)) emit_sketch_bf16(B, x, all, sp, S, W, o.precision == TTC_PREC_TF32);
+      else emit_sketch_f64(B, x, all, sp, S, W);
+    }
     B.stage(1);
     std::vector<std::vector<int>> eff;
     emit_rand_sweep(B, x, y, all, sp, W, rho_all, after == nullptr, &eff);

@@ -420,6 +420,45 @@ def test_batched_round_rand_then_svd():
             assert rel(got, ref) < (1e-10 if prec == "fp64" else 1e-7)
 
 
+def _range_finder_forms(dims, rep, s):
+    """Forms the randomized sweep's range finder takes per bond (F: the sketch rank s is below
+    both dimensions of y_k's unfolding; T: r_{k+1} is the smallest; W: n e_k is)."""
+    e, forms = 1, []
+    for k in range(len(dims) - 1):
+        m, c = dims[k] * e, rep[k + 1]
+        q = min(m, c, s[k + 1])
+        forms.append("F" if q == s[k + 1] else ("T" if q == c else "W"))
+        e = q
+    return forms
+
+
+@pytest.mark.parametrize("prec", ["fp64", "bf16"])
+def test_batched_round_rand_then_svd_mixed_levels(prec):
+    """A batch whose range finders take all three forms.  With the SVD sweep following, the
+    compressing levels (F) read the sketch and the others take the reduced forms that keep only
+    range(Q).  x = t + t/2 represents t at twice its ranks, and the sketch ranks of the F levels
+    cover t's ranks, so the result is t rounded, whatever the sketch's precision."""
+    dims = (2,) * 10
+    rks = [1, 2, 4, 8, 8, 16, 16, 16, 8, 4, 1]
+    block = 8
+    s = ttcuda._sketch_ranks(dims, rks, block)
+    g = np.random.default_rng(77)
+    xs, forms = [], set()
+    for r in (5, 6, 3):
+        t = o.rand_tt(dims, o.r_and_d_to_rks([1] + [r] * 9 + [1], dims), g)
+        x = o.tt_add(t, o.tt_scale(0.5, t))
+        forms.update(_range_finder_forms(dims, x.ttv_rks, s))
+        xs.append(x)
+    assert forms == {"F", "T", "W"}
+    xb = ttcuda.DeviceBatch.from_tts([to_dev(x) for x in xs])
+    yb = ttcuda.DeviceBatch(dims, [ttcuda._rand_out_caps(dims, s)] * len(xs))
+    xb.round_rand(yb, rks, orthogonal=False, seed=21, block_rks=block, precision=prec, after_tol=1e-10)
+    for x, got in zip(xs, yb.download()):
+        ref = o.tt_rounding(o.ttrand_rounding(x, rks, orthogonal=False, seed=21, block_rks=block), tol=1e-10)
+        assert got.ttv_rks == ref.ttv_rks == o.tt_rounding(x, tol=1e-10).ttv_rks
+        assert rel(got, ref) < 1e-10
+
+
 # ------------------------------------------------------ mixed precision on non-minimal TTs
 @pytest.mark.parametrize("block", [None, 8, 16, 64])
 @pytest.mark.parametrize("orthogonal", [False, True])
