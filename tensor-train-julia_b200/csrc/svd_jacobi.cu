@@ -1172,8 +1172,11 @@ static int jacobi_block_csize(int count, int max_n, size_t smem, bool ordered) {
   int c = std::max(1, slots / std::max(1, count));
   if (ordered) c = std::max(c, per_sm >= 2 ? 8 : 4);
   c = std::min(c, std::min(8, pairs));
+  // a power of two, rounded up when the launch is ordered: a problem whose block pairs outnumber
+  // its CTAs takes two visits per round, which doubles its latency
   int p2 = 1;
-  while (p2 * 2 <= c) p2 *= 2;
+  if (ordered) while (p2 < c) p2 *= 2;
+  else while (p2 * 2 <= c) p2 *= 2;
   return p2;
 }
 
