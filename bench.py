@@ -9,7 +9,10 @@ One step rounds the whole batch to tol = 1e-8 in two variants:
   * mixed : ttrand_rounding with a Gaussian sketch whose contractions run in BF16 on the
             tcgen05 tensor cores (FP32 accumulation), sketch ranks = default_rank_heuristic
             (r + ceil(max r / 2)), FP64 range finder / projection, then the FP64 truncated-SVD
-            sweep tt_rounding(tol);                         -> `value`
+            sweep tt_rounding(tol) (no range finder of this workload compresses, so the library
+            plans no sketch: see `range_finder_levels_compressing`);   -> `value`
+  * rank_limited: the same batch rounded to rank 64 (ttrand_rounding(y, 64) + SVD sweep against
+            tt_rounding(rmax = 64)), where every interior range finder compresses;
   * fp64  : deterministic tt_rounding(tol) (FP64 QR sweep + truncated-SVD sweep) -> `fp64`.
 `value` is whole-job roundings/s with the inputs resident in HBM (device events around K
 replays of the captured plan); `e2e` is the same metric through the C ABI with host buffers
@@ -35,11 +38,18 @@ sys.path.insert(0, os.path.join(ROOT, "tensor-train-julia_b200"))
 
 D, NPHYS, BATCH, RMIN, RMAX, TOL = 32, 2, 64, 16, 256, 1e-8
 METRIC = "TT roundings/s at d=32,r=256: mixed vs FP64 GPU at 1e-8 rel err; % roofline"
-# DRAM bytes (read + write) per launch of the QR family (householder_qr_kernel and
-# householder_apply_q_kernel, 123 launches) in one mixed step of the 64-TT workload, mean over the
-# launches of an ncu capture of that step (dram__bytes_read.sum + dram__bytes_write.sum): 99.7 GB
-# over 123 launches.  Other batch sizes change the L2 residency, so no scaled figure is given.
-QR_FAMILY_DRAM_BYTES_PER_LAUNCH_64TT = 810.7e6
+# DRAM bytes (read + write) per launch of the step's two large kernels, from ncu section captures
+# (dram__bytes_read.sum + dram__bytes_write.sum) of smaller cases of the same kernels, scaled to a
+# 64-TT launch by the problems it holds (the factors stay in L2 within a launch, so a launch reads
+# its inputs once and traffic grows with the problem count):
+#  * householder_qr_kernel: 7.57 MB for a 32-TT orthogonalisation-sweep launch at bond 12
+#    (unfoldings up to 512 x 256) -> 15.1 MB for 64 TTs;
+#  * jacobi_svd (the Gram-block kernel): 33.75 MB for 64 preconditioned 256 x 256 factors
+#    (bench.py --jacobi-bench), the largest launch of the SVD sweep.
+DOMINANT_DRAM_BYTES_PER_LAUNCH_64TT = {
+    "householder_qr": (15.1e6, "ncu capture of a 32-TT orthogonalisation-sweep QR launch (bond 12), x2 for 64 TTs"),
+    "jacobi_svd": (33.75e6, "ncu capture of a 64-problem 256 x 256 launch (bench.py --jacobi-bench), the largest"),
+}
 
 
 # ------------------------------------------------------------------------- workload
@@ -835,11 +845,11 @@ def main():
                              "fp64_algorithmic": flops_fp64 * world * args.steps / (ms_fp64 / 1e3) / 1e9},
             "roofline": {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": fp64_peak_tflops,
                          "unit": "TFLOP/s", "frac": (achieved / fp64_peak_tflops) if achieved else None,
-                         "traffic": (QR_FAMILY_DRAM_BYTES_PER_LAUNCH_64TT
-                                     if dom == "householder_qr" and len(tts) == 64 else None),
-                         "traffic_note": "mean dram read+write per QR-family launch of one 64-TT mixed step (ncu "
-                                         "capture of that step); the 768-row randomized-sweep QRs carry it: "
-                                         "input and Q exceed L2",
+                         "traffic": (DOMINANT_DRAM_BYTES_PER_LAUNCH_64TT[dom][0]
+                                     if dom in DOMINANT_DRAM_BYTES_PER_LAUNCH_64TT and len(tts) == 64 else None),
+                         "traffic_note": (DOMINANT_DRAM_BYTES_PER_LAUNCH_64TT[dom][1] + "; far below the launch's "
+                                          "algorithmic bytes: latency-bound, the factors stay in L2"
+                                          if dom in DOMINANT_DRAM_BYTES_PER_LAUNCH_64TT else None),
                          "peak_source": "FP64 torch.matmul (cuBLAS DGEMM) 4096^3, best of 10, measured in this run "
                                         "(MEASURED_PEAKS.json has no FP64 entry)",
                          "avg_launch_ms": dom_avg_ms, "launches_per_step": dom_n,
