@@ -625,6 +625,16 @@ __device__ __forceinline__ void rotate_block(const RotA& A, const RotA& B, doubl
   }
 }
 
+// rotate_block without branches: a pair that does not rotate has c = 1, s = 0 exactly, which leaves
+// finite entries unchanged bit for bit.
+__device__ __forceinline__ void rotate_block_nb(const RotA& A, const RotA& B, double& b00, double& b01, double& b10,
+                                                double& b11) {
+  const double u0 = A.c * b00 - A.s * b10, v0 = fma(A.s, b00, A.c * b10);
+  const double u1 = A.c * b01 - A.s * b11, v1 = fma(A.s, b01, A.c * b11);
+  b00 = B.c * u0 - B.s * u1; b01 = fma(B.s, u0, B.c * u1);
+  b10 = B.c * v0 - B.s * v1; b11 = fma(B.s, v0, B.c * v1);
+}
+
 // V's rows in registers (thread = row): the rotations of inner round R, whose slots are known at
 // compile time, applied to the row.
 __host__ __device__ constexpr int rr_slot(int pos, int round) { return pos == 0 ? 0 : ((pos - 1 + round) % 31) + 1; }
@@ -680,7 +690,7 @@ __device__ __forceinline__ void v_round(double (&v)[32], const RotA* P, int r) {
 template <bool FULL>
 __device__ __forceinline__ void gram_round(double* G, double (&vrow)[32], const RotA* cA, const RotB* cB, RotA* nA,
                                            RotB* nB, const unsigned char* blk, const unsigned long long* sched, int r, int nr,
-                                           const RotCfg& q, int* s_rot) {
+                                           const RotCfg& q, int* s_rot, unsigned long long& pre) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp < 3 || (warp == 4 && lane < 24)) {
     const int bk = warp < 3 ? tid : 96 + lane;
@@ -712,7 +722,8 @@ __device__ __forceinline__ void gram_round(double* G, double (&vrow)[32], const 
       // block update's orientation), whose slots (Ai, Aj), (Bi, Bj) the schedule fixes
       int ia, ib, Ai, Aj, Bi, Bj, u, v;
       if (FULL) {
-        const unsigned long long e = sched[(r + 1) * 16 + p];
+        const unsigned long long e = pre;   // schedule entry of round r + 1, loaded a round earlier
+        if (r + 2 < nr) pre = sched[(r + 2) * 16 + p];
         ia = e & 15; ib = (e >> 4) & 15; Ai = (e >> 8) & 31; Aj = (e >> 13) & 31;
         Bi = (e >> 18) & 31; Bj = (e >> 23) & 31; u = (e >> 28) & 31; v = (e >> 33) & 31;
       } else {
@@ -727,12 +738,11 @@ __device__ __forceinline__ void gram_round(double* G, double (&vrow)[32], const 
       double b10 = G[Aj + Bi * GLD], b11 = G[Aj + Bj * GLD];
       const RotA A = cA[ia], B = cA[ib];
       const RotB AB = cB[ia], BB = cB[ib];
-      rotate_block(A, B, b00, b01, b10, b11);
+      rotate_block_nb(A, B, b00, b01, b10, b11);
+      // a pair that does not rotate has t = 0: its diagonal stays as it is
       const double guv = (u == Ai) ? ((v == Bi) ? b00 : b01) : ((v == Bi) ? b10 : b11);
-      const double guu = !A.on ? ((u == Ai) ? AB.gii : AB.gjj)
-                               : ((u == Ai) ? AB.gii - AB.t * AB.gij : AB.gjj + AB.t * AB.gij);
-      const double gvv = !B.on ? ((v == Bi) ? BB.gii : BB.gjj)
-                               : ((v == Bi) ? BB.gii - BB.t * BB.gij : BB.gjj + BB.t * BB.gij);
+      const double guu = (u == Ai) ? AB.gii - AB.t * AB.gij : AB.gjj + AB.t * AB.gij;
+      const double gvv = (v == Bi) ? BB.gii - BB.t * BB.gij : BB.gjj + BB.t * BB.gij;
       if (set_pair(nA[p], nB[p], u, v, guu, gvv, guv, q)) *s_rot = 1;
     }
   }
@@ -908,14 +918,15 @@ __global__ void __launch_bounds__(NT, 2)
           double vrow[32];
 #pragma unroll
           for (int c = 0; c < 32; ++c) vrow[c] = (c == lane) ? 1.0 : 0.0;
+          unsigned long long pre = (warp == 3 && lane < 16) ? s_sched[16 + lane] : 0ull;
           if (full) {
             for (int r = 0; r < 31; ++r)
               gram_round<true>(G, vrow, s_ra[r & 1], s_rb[r & 1], s_ra[(r + 1) & 1], s_rb[(r + 1) & 1], s_blk, s_sched,
-                               r, 31, q, &s_rot);
+                               r, 31, q, &s_rot, pre);
           } else {
             for (int r = 0; r < 16; ++r)
               gram_round<false>(G, vrow, s_ra[r & 1], s_rb[r & 1], s_ra[(r + 1) & 1], s_rb[(r + 1) & 1], s_blk,
-                                s_sched, r, 16, q, &s_rot);
+                                s_sched, r, 16, q, &s_rot, pre);
           }
           if (warp == 6) {
 #pragma unroll

@@ -211,7 +211,8 @@ def bf16_round(x):
     return np.ldexp(np.round(m * 256.0) / 256.0, e)
 
 
-@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (128, 128, 64), (200, 130, 100), (513, 257, 264), (40, 300, 8)])
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (128, 128, 64), (200, 130, 100), (513, 257, 264), (40, 300, 8),
+                                   (2048, 2400, 200)])
 def test_bf16_tcgen05_gemm(ctx, m, n, k):
     g = np.random.default_rng(m + 3 * n + 7 * k)
     A = g.standard_normal((m, k))
@@ -229,7 +230,8 @@ def test_bf16_tcgen05_gemm(ctx, m, n, k):
     assert np.linalg.norm(got - ref) <= 1e-6 * np.linalg.norm(ref)
 
 
-@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (128, 128, 32), (200, 130, 100), (513, 257, 266), (40, 300, 4)])
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (128, 128, 32), (200, 130, 100), (513, 257, 266), (40, 300, 4),
+                                   (2048, 2400, 200)])
 def test_tf32_tcgen05_gemm(ctx, m, n, k):
     """kind::tf32: FP32 operands read with a 10-bit mantissa (each operand's relative error
     below 2^-10, so a product's below 2^-9), FP32 accumulation."""
