@@ -122,7 +122,12 @@ struct ApplyDesc {
   double* Y;         // internal TT core  ((R r), n_out, (R' r')) col-major, R index fastest
   int R, Rn, r, rn, n;
 };
-void launch_apply(const ApplyDesc* d, int count, long long max_elems, cudaStream_t s);
+// one CTA per right rank index nu' of each problem: grid (max rn, count).  Staged in shared memory:
+// V[:, :, nu'] and, one a' at a time, H[:, :, :, a'].
+__host__ __device__ inline long long apply_smem_doubles(const ApplyDesc& d) {
+  return (long long)d.n * d.r + (long long)d.n * d.n * d.R;
+}
+void launch_apply(const ApplyDesc* d, int count, int max_rn, int max_smem_doubles, cudaStream_t s);
 
 // ---- Philox sketch generation (tt_kernels.cu): Gaussian block entries
 // dst (Julia layout of the block, flat index e) = scale * N(0,1)_{seed, stream, e}.

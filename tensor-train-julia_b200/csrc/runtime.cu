@@ -154,7 +154,7 @@ static void launch_op(ttc_context* c, const Plan& p, const Op& op) {
       case OP_COPY: launch_copy((const CopyDesc*)d, op.count, op.total, s); break;
       case OP_ZERO: launch_zero((const ZeroDesc*)d, op.count, op.total, s); break;
       case OP_SUMSQ: launch_sumsq((const NormDesc*)d, op.count, s); break;
-      case OP_APPLY: launch_apply((const ApplyDesc*)d, op.count, op.total, s); break;
+      case OP_APPLY: launch_apply((const ApplyDesc*)d, op.count, op.a, op.b, s); break;
       case OP_GEMM32: launch_gemm_f32((const GemmDesc*)d, op.count, op.total, s); break;
       case OP_CVT32: launch_cvt_f32((const CvtDesc*)d, op.count, op.total, s); break;
       case OP_WIDEN: launch_widen((const CvtDesc*)d, op.count, op.total, s); break;
@@ -609,14 +609,20 @@ void Builder::sumsq(const std::vector<NormDesc>& v) {
 void Builder::apply(const std::vector<ApplyDesc>& v) {
   if (v.empty()) return;
   long long mx = 0;
+  int max_rn = 0;
+  long long max_sm = 0;
   for (auto& d : v) {
     mx = std::max(mx, (long long)d.R * d.r * d.n * d.Rn * d.rn);
+    max_rn = std::max(max_rn, d.rn);
+    max_sm = std::max<long long>(max_sm, apply_smem_doubles(d));
     const bool on = wsbase != nullptr;
     chk(on, d.H, (long long)d.R * d.n * d.n * d.Rn, 8, "apply H");
     chk(on, d.V, (long long)d.r * d.n * d.rn, 8, "apply V");
     chk(on, d.Y, (long long)d.R * d.r * d.n * d.Rn * d.rn, 8, "apply Y");
   }
   Op op; op.kind = OP_APPLY; op.off = plan->push(v); op.count = (int)v.size(); op.total = mx;
+  TTC_REQUIRE(max_sm <= 25600, TTC_EDIM, "apply: operator and vector ranks too large for the staged slices");
+  op.a = max_rn; op.b = (int)max_sm;
   plan->ops.push_back(op);
 }
 void Builder::philox(const std::vector<PhiloxDesc>& v) {

@@ -190,37 +190,67 @@ void launch_select(const SelectDesc* d, int count, int max_rows, int max_cols, c
 
 // ---------------------------------------------------------------- MPO x TT apply
 // Y[(a + R*nu), i, (a' + R'*nu')] = sum_j H[a, i, j, a'] * V[nu, j, nu'] (internal layouts;
-// src/tt_operations.jl:184).  One thread per output element, consecutive threads on the
-// fastest output index a, so H is read coalesced and V is a broadcast.  HBM-bound on Y.
-// Output element e = u + U w with u = a + R nu (the combined left rank index, operator index
-// fastest) and w = i + n (an + R' nun): consecutive threads write consecutive elements, and each
-// reads its n operator entries and n vector entries (shared by the R threads of one nu and the r
-// threads of one a, so they come from L1).  The HBM traffic is the output's write stream.
-template <typename I>
+// src/tt_operations.jl:184).  HBM-bound on the output's write stream: the output core is R R'
+// times the input core, and H and V are read a few times over from L2.
+// Output column w = i + n (a' + R' nu') is a contiguous run of U = R r elements (u = a + R nu).  A
+// CTA takes one nu' of one problem: it stages V[:, :, nu'] (n r values) in shared memory once, then
+// for each (a', i) the n R operator entries H[:, i, :, a'], and writes the n R' columns of that nu'
+// with consecutive threads on consecutive u (coalesced stores).  Each thread follows its (a, nu)
+// through the column by constant increments (the block size divided by R), with no division per
+// element; an element costs 2n shared-memory loads, n FMAs and one store.
 __global__ void apply_kernel(const ApplyDesc* __restrict__ descs) {
+  extern __shared__ double asm_[];
   const ApplyDesc D = descs[blockIdx.y];
-  const I R = (I)D.R, n = (I)D.n, Rn = (I)D.Rn;
-  const I U = R * (I)D.r;
-  const I total = U * n * Rn * (I)D.rn;
-  const long long hj = (long long)D.R * D.n;          // H stride of j
-  for (I e = (I)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (I)gridDim.x * blockDim.x) {
-    const I u = e % U, w = e / U;
-    const I nu = u / R, a = u - nu * R;
-    const I i = w % n, t = w / n;
-    const I an = t % Rn, nun = t / Rn;
-    const double* h = D.H + a + (long long)R * i + hj * n * (long long)an;
-    const double* v = D.V + nu + (long long)D.r * n * (long long)nun;
-    double acc = 0.0;
-    for (int j = 0; j < D.n; ++j) acc = fma(h[hj * j], v[(long long)D.r * j], acc);
-    D.Y[e] = acc;
+  const int nun = blockIdx.x;
+  if (nun >= D.rn) return;                         // uniform: the launch covers the largest rn
+  const int R = D.R, n = D.n, Rn = D.Rn, r = D.r;
+  const long long U = (long long)R * r;
+  double* vs = asm_;                               // vs[j r + nu] = V[nu, j, nu']
+  double* hs = asm_ + (size_t)n * r;               // hs[a + R (i + n j)] = H[a, i, j, a'] of one a'
+  for (int e = threadIdx.x; e < n * r; e += blockDim.x) {
+    const int j = e / r, nu = e - j * r;
+    vs[e] = D.V[nu + (long long)r * (j + (long long)n * nun)];
+  }
+  const int stA = blockDim.x % R, stNu = blockDim.x / R;
+  const int a0 = threadIdx.x % R, nu0 = threadIdx.x / R;
+  const long long cstride = U;                     // output column i + 1 follows column i
+  for (int an = 0; an < Rn; ++an) {
+    __syncthreads();                               // the previous a's reads of hs are done
+    const double* hsrc = D.H + (long long)R * n * n * an;   // H[:, :, :, a'] is contiguous
+    for (int e = threadIdx.x; e < R * n * n; e += blockDim.x) hs[e] = hsrc[e];
+    __syncthreads();
+    // the n columns (i = 0 .. n-1) of this a' and nu' together: vs is read once per (u, j)
+    double* y = D.Y + U * (long long)n * (an + (long long)Rn * nun);
+    int a = a0, nu = nu0;
+    for (long long u = threadIdx.x; u < U; u += blockDim.x) {
+      if (n == 2) {
+        const double v0 = vs[nu], v1 = vs[r + nu];
+        y[u] = fma(hs[a + 2 * R], v1, hs[a] * v0);
+        y[u + cstride] = fma(hs[a + 3 * R], v1, hs[a + R] * v0);
+      } else {
+        for (int i = 0; i < n; ++i) {
+          double acc = 0.0;
+          for (int j = 0; j < n; ++j) acc = fma(hs[a + R * (i + n * j)], vs[j * r + nu], acc);
+          y[u + cstride * i] = acc;
+        }
+      }
+      a += stA; nu += stNu;
+      if (a >= R) { a -= R; ++nu; }
+    }
   }
 }
 
-void launch_apply(const ApplyDesc* d, int count, long long max_elems, cudaStream_t s) {
-  if (count <= 0 || max_elems <= 0) return;
-  const long long blocks = std::min<long long>((max_elems + NT - 1) / NT, 148LL * 16);
-  if (max_elems < (1LL << 31)) apply_kernel<unsigned><<<dim3((unsigned)blocks, (unsigned)count), NT, 0, s>>>(d);
-  else apply_kernel<unsigned long long><<<dim3((unsigned)blocks, (unsigned)count), NT, 0, s>>>(d);
+void launch_apply(const ApplyDesc* d, int count, int max_rn, int max_smem_doubles, cudaStream_t s) {
+  if (count <= 0 || max_rn <= 0) return;
+  const size_t smem = sizeof(double) * (size_t)std::max(1, max_smem_doubles);
+  TTC_REQUIRE(smem <= 200 * 1024, TTC_EDIM, "apply: operator and vector ranks too large for the staged slices");
+  static PerDeviceOnce attr_once;
+  int dev = 0;
+  TTC_CUDA(cudaGetDevice(&dev));
+  attr_once.run(dev, [] {
+    TTC_CUDA(cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  });
+  apply_kernel<<<dim3((unsigned)max_rn, (unsigned)count), NT, smem, s>>>(d);
   TTC_CHECK_LAUNCH();
 }
 
