@@ -516,6 +516,7 @@ size_t qr_smem(int max_m) {
   return sizeof(double) * (NB * NB * 4 + 3 * NB + NW + 2 + NW * 128 + (size_t)(max_m + 15) * NB);
 }
 
+constexpr int kQrWaves = 2;
 void launch_qr_cfg(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags) {
   const size_t smem = qr_smem(max_m);
   static PerDeviceOnce attr_once;
@@ -526,11 +527,12 @@ void launch_qr_cfg(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, 
                                   (int)qr_smem(QR_MAX_M)));
   });
   const int nsm = current_sm_count();
-  // CTAs per problem: fill the resident-CTA slots of the GPU, at most 8 (portable cluster)
+  // CTAs per problem: up to two waves of the resident-CTA slots of the GPU (the planner puts the
+  // largest problems first, so the second wave holds the short ones), at most 8 (portable cluster)
   int per_sm = 1;
   TTC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, householder_qr_kernel, NT, smem));
   const int slots = nsm * std::max(1, per_sm);
-  int c = std::min(8, std::max(1, slots / count));
+  int c = std::min(8, std::max(1, kQrWaves * slots / count));
   int csize = 1;
   while (csize * 2 <= c) csize *= 2;
   cudaLaunchConfig_t cfg{};

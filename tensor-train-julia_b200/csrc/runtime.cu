@@ -504,8 +504,14 @@ void Builder::qr(const std::vector<QRDesc>& v) {
     TTC_REQUIRE(d.lda >= d.m && (!d.Q || d.ldq >= d.m) && (!d.R || d.ldr >= (d.r_trans ? d.n : K)), TTC_EINTERNAL,
                 "qr: leading dims");
   }
-  Op op; op.kind = OP_QR; op.off = plan->push(v); op.count = (int)v.size(); op.a = mm; op.b = nn;
-  for (auto& d : v) op.flops += qr_flops(d.m, d.n, d.Q != nullptr);
+  // largest problems first (the hardware starts clusters in index order): a launch whose
+  // clusters outnumber the resident slots runs the long problems in the first wave
+  std::vector<QRDesc> w(v);
+  std::stable_sort(w.begin(), w.end(), [](const QRDesc& a, const QRDesc& b) {
+    return qr_flops(a.m, a.n, a.Q != nullptr) > qr_flops(b.m, b.n, b.Q != nullptr);
+  });
+  Op op; op.kind = OP_QR; op.off = plan->push(w); op.count = (int)w.size(); op.a = mm; op.b = nn;
+  for (auto& d : w) op.flops += qr_flops(d.m, d.n, d.Q != nullptr);
   plan->ops.push_back(op);
 }
 void Builder::qapply(const std::vector<QApplyDesc>& v) {
