@@ -644,7 +644,10 @@ __device__ __forceinline__ void v_apply(double (&v)[32], const RotA* P) {
   // without a branch and all sixteen loads are issued first
   double c[16], s[16];
 #pragma unroll
-  for (int p = 0; p < 16; ++p) { c[p] = P[p].c; s[p] = P[p].s; }
+  for (int p = 0; p < 16; ++p) {   // (c, s) are the first 16 bytes of a 16-byte aligned RotA
+    const double2 cs = *reinterpret_cast<const double2*>(&P[p].c);
+    c[p] = cs.x; s[p] = cs.y;
+  }
 #pragma unroll
   for (int p = 0; p < 16; ++p) {
     const int x = FULL ? rr_slot(p, R) : p, y = FULL ? rr_slot(31 - p, R) : 16 + ((p + R) & 15);
