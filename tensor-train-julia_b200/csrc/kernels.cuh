@@ -36,6 +36,7 @@ struct QRDesc {
   // zero; the factorization runs on the bounded block (Q and R keep their full shapes)
   const int* m_dev; int m_mult;
   const int* n_dev; int n_mult;
+  double* Rt; int ldrt;   // optional second copy of R, transposed: R^T[j][i] at Rt[i*ldrt + j]
 };
 constexpr int QR_MAX_M = 1536;
 void launch_qr(const QRDesc* d_descs, int count, int max_m, cudaStream_t s, int* d_flags);

@@ -442,6 +442,7 @@ __global__ void __launch_bounds__(NT, 1) householder_qr_kernel(const QRDesc* __r
         const double v = (i <= j) ? A[(long long)j * lda + i] : 0.0;
         if (D.r_trans) D.R[(long long)i * D.ldr + j] = v;
         else D.R[(long long)j * D.ldr + i] = v;
+        if (D.Rt) D.Rt[(long long)i * D.ldrt + j] = v;
       }
   }
   if (!D.Q) return;

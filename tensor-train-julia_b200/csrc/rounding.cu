@@ -103,9 +103,21 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
   const int N = y->N;
   const size_t T = tts.size();
   if (T == 0) return;
+  // The product T2 = core(j-1) T1 of bond j has core j-1's layout (ld n_{j-1} capr(j-1)) and is
+  // zero beyond the kept rank, so bond j-1 reads it in place of core j-1, which it rewrites
+  // anyway; only the last bond's product is copied into core 0.  Two buffers per TT alternate.
+  const size_t mark0 = B.mark();
+  std::vector<double*> T2buf[2] = {std::vector<double*>(T), std::vector<double*>(T)};
+  for (size_t i = 0; i < T; ++i) {
+    size_t mx = 1;
+    for (int j = N - 1; j >= 1; --j)
+      mx = std::max(mx, (size_t)y->capr(tts[i], j - 1) * (size_t)y->dims[j - 1] * (size_t)rp[i][j]);
+    T2buf[0][i] = B.wd(mx);
+    T2buf[1][i] = B.wd(mx);
+  }
   for (int j = N - 1; j >= 1; --j) {
     const size_t mk = B.mark();
-    std::vector<CopyDesc> cpX, cpY, cpR, cpW, cpT2;
+    std::vector<CopyDesc> cpX, cpR, cpW, cpT2;
     std::vector<QRDesc> qr, qr2;
     std::vector<JacobiDesc> jac;
     std::vector<TruncDesc> tr;
@@ -128,7 +140,9 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
       int* info = infos + i;
       double* X = B.wd((size_t)p * q);
       double* T1 = B.wd((size_t)q * q);
-      double* T2 = B.wd((size_t)ml * q);
+      double* T2 = T2buf[j & 1][i];
+      // core j as this bond reads it: the previous bond's product (core j is rewritten below)
+      const double* Cj = (j == N - 1) ? y->core(t, j) : T2buf[(j + 1) & 1][i];
       if (p >= q) {
         // M^T = Q R1 (Householder), R1^T = Q2 R2, one-sided Jacobi on R2^T = R1 Q2: same left
         // singular vectors as R1 in about half the sweeps (QR-LQ preconditioning); the factor
@@ -142,9 +156,8 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         double* Tws = B.wd(qr_tws(p, q));
         double* Tws2 = B.wd(qr_tws(q, q));
         double* Bq = B.wd((size_t)p * q);           // [U; 0], then Q [U; 0]
-        cpX.push_back(cd2(y->core(t, j), X, q, p, 1, yc, p, 1));
-        qr.push_back({p, q, X, p, nullptr, 0, R, q, Tws, 0, rk1, n, nullptr, 0});
-        cpY.push_back(cd2(R, Y, q, q, 1, q, q, 1));
+        cpX.push_back(cd2(Cj, X, q, p, 1, yc, p, 1));
+        qr.push_back({p, q, X, p, nullptr, 0, R, q, Tws, 0, rk1, n, nullptr, 0, Y, q});   // and Y = R1^T
         // R1 has rows >= n r' zero, so R1^T has those columns zero and R2^T those rows
         qr2.push_back({q, q, Y, q, nullptr, 0, Rc, q, Tws2, 1, nullptr, 0, rk1, n});   // R2^T into Rc
         jac.push_back({q, q, Rc, q, nullptr, 0, sig, perm, info, rk1, n});
@@ -165,23 +178,22 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         int* perm = B.wi(p);
         double* Tws = B.wd(qr_tws(q, p));
         double* Vt = B.wd((size_t)p * q);
-        cpX.push_back(cd2(y->core(t, j), X, q, p, 1, yc, 1, q));
+        cpX.push_back(cd2(Cj, X, q, p, 1, yc, 1, q));
         qr.push_back({q, p, X, q, nullptr, 0, R, p, Tws, 0, nullptr, 0, rk1, n});   // columns >= n r' zero
         cpR.push_back(cd2(R, Rc, p, p, p, 1, 1, p));          // Rc = R1^T
         jac.push_back({p, p, Rc, p, nullptr, 0, sig, perm, info, rk1, n});   // rows >= n r' zero
         tr.push_back({sig, perm, p, rank});
         sel.push_back({Rc, p, sig, perm, rank, p, q, p, Vt, p, 1});
         cpW.push_back(cd2(Vt, y->core(t, j), p, q, 1, p, yc, 1));
-        g2.push_back(gd(q, q, p, y->core(t, j), 1, yc, Vt, 1, p, T1, 1, q));   // M V (before core j changes)
+        g2.push_back(gd(q, q, p, Cj, 1, yc, Vt, 1, p, T1, 1, q));   // M V
         g2.back().n_dev = rank;                       // Vt is zero beyond the kept rank
       }
       g3.push_back(gd(ml, q, q, y->core(t, j - 1), 1, ml, T1, 1, q, T2, 1, ml));
       g3.back().n_dev = rank;                         // T1 is zero beyond the kept rank
-      cpT2.push_back(cd2(T2, y->core(t, j - 1), ml, q, 1, ml, 1, ml));
+      if (j == 1) cpT2.push_back(cd2(T2, y->core(t, j - 1), ml, q, 1, ml, 1, ml));
     }
     B.copy(cpX);
     B.qr(qr);
-    B.copy(cpY);
     B.qr(qr2);
     B.copy(cpR);
     B.jacobi(jac);
@@ -195,6 +207,7 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
     B.copy(cpT2);
     B.release(mk);
   }
+  B.release(mark0);
 }
 
 // Early exit of _tt_rounding (src/tt_rounding.jl:179-181): norm(core N) < tol.

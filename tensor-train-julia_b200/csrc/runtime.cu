@@ -498,6 +498,8 @@ void Builder::qr(const std::vector<QRDesc>& v) {
     chk(on, d.A, (long long)d.lda * (d.n - 1) + d.m, 8, "qr A");
     if (d.Q) chk(on, d.Q, (long long)d.ldq * (K - 1) + d.m, 8, "qr Q");
     if (d.R) chk(on, d.R, d.r_trans ? (long long)d.ldr * (K - 1) + d.n : (long long)d.ldr * (d.n - 1) + K, 8, "qr R");
+    if (d.Rt) chk(on, d.Rt, (long long)d.ldrt * (K - 1) + d.n, 8, "qr R^T");
+    TTC_REQUIRE(!d.Rt || (d.R && d.ldrt >= d.n), TTC_EINTERNAL, "qr: the transposed copy of R needs R");
     if (d.Tws) chk(on, d.Tws, (long long)((K + 15) / 16) * 256, 8, "qr Tws");
     TTC_REQUIRE(d.m <= QR_MAX_M, TTC_EDIM, "qr: row count exceeds the supported maximum (1536)");
     TTC_REQUIRE(!d.Q || d.Tws, TTC_EINTERNAL, "qr: forming Q needs the block-reflector workspace");
