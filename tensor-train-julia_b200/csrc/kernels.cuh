@@ -94,6 +94,7 @@ struct SelectDesc {
   int src_cols;              // columns of X (perm entries are < src_cols)
   double* U; int ldu;
   int scale;                 // 1: divide by sigma; 0: copy; 2: multiply by sigma
+  int zrows;                 // when above rows: rows [rows, zrows) of every output column are zeroed
 };
 void launch_select(const SelectDesc* d, int count, int max_rows, int max_cols, cudaStream_t s);
 

@@ -69,12 +69,16 @@ void emit_orth_left(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<in
       const int a = rp[i][j], an = rp[i][j + 1];
       const int xr0 = x->rk(t, j), xr1 = x->rk(t, j + 1), xc = x->capr(t, j), yc = y->capr(t, j);
       double* C = B.wd((size_t)a * n * xr1);
-      double* Q = B.wd((size_t)a * n * an);
       double* Tws = B.wd(qr_tws(a * n, xr1));
       const double* A = (j == 0) ? B.ctx->d_one : FR[i];
       g.push_back(gd(a, n * xr1, xr0, A, 1, a, x->core(t, j), 1, xc, C, 1, a));
-      q.push_back({a * n, xr1, C, a * n, Q, a * n, FRn[i], an, Tws});
-      cp.push_back(cd3(Q, y->core(t, j), a, n, an, 1, a, (long long)a * n, 1, yc, (long long)yc * n));
+      if (yc == a) {   // core j of y has Q's layout (a n rows, column stride a n): Q is written there
+        q.push_back({a * n, xr1, C, a * n, y->core(t, j), a * n, FRn[i], an, Tws});
+      } else {
+        double* Q = B.wd((size_t)a * n * an);
+        q.push_back({a * n, xr1, C, a * n, Q, a * n, FRn[i], an, Tws});
+        cp.push_back(cd3(Q, y->core(t, j), a, n, an, 1, a, (long long)a * n, 1, yc, (long long)yc * n));
+      }
     }
     B.gemm(g);
     B.qr(q);
@@ -117,13 +121,12 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
   }
   for (int j = N - 1; j >= 1; --j) {
     const size_t mk = B.mark();
-    std::vector<CopyDesc> cpX, cpR, cpW, cpT2;
+    std::vector<CopyDesc> cpX, cpW, cpT2;
     std::vector<QRDesc> qr, qr2;
     std::vector<JacobiDesc> jac;
     std::vector<TruncDesc> tr;
     std::vector<SelectDesc> sel;
     std::vector<GemmDesc> g2, g3;
-    std::vector<ZeroDesc> zb;
     std::vector<QApplyDesc> qa;
     int* infos = B.diag_ints((int)T);
     const int n = (int)y->dims[j], nl = (int)y->dims[j - 1];
@@ -162,8 +165,7 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         qr2.push_back({q, q, Y, q, nullptr, 0, Rc, q, Tws2, 1, nullptr, 0, rk1, n});   // R2^T into Rc
         jac.push_back({q, q, Rc, q, nullptr, 0, sig, perm, info, rk1, n});
         tr.push_back({sig, perm, q, rank});
-        zb.push_back({Bq, (long long)p * q});
-        sel.push_back({Rc, q, sig, perm, rank, q, q, q, Bq, p, 1});
+        sel.push_back({Rc, q, sig, perm, rank, q, q, q, Bq, p, 1, p});   // [U; 0]: rows q .. p-1 zeroed
         g2.push_back(gd(q, q, q, R, q, 1, Bq, 1, p, T1, 1, q));
         g2.back().n_dev = rank;                       // U is zero beyond the kept rank
         qa.push_back({p, q, X, p, Tws, Bq, p, q, rank, rk1, n});
@@ -172,15 +174,14 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
         // M = Q1 R1 (q > p, Q1 not formed); one-sided Jacobi on R1^T (p x p) gives V Sigma
         // in its columns: core j <- V^T (normalised columns, exactly orthonormal up to the
         // rotation threshold), and the factor absorbed into core j-1 is M V = U Sigma.
-        double* R = B.wd((size_t)p * p);
         double* Rc = B.wd((size_t)p * p);
         double* sig = B.wd(p);
         int* perm = B.wi(p);
         double* Tws = B.wd(qr_tws(q, p));
         double* Vt = B.wd((size_t)p * q);
         cpX.push_back(cd2(Cj, X, q, p, 1, yc, 1, q));
-        qr.push_back({q, p, X, q, nullptr, 0, R, p, Tws, 0, nullptr, 0, rk1, n});   // columns >= n r' zero
-        cpR.push_back(cd2(R, Rc, p, p, p, 1, 1, p));          // Rc = R1^T
+        // columns >= n r' zero; R1 written transposed: Rc = R1^T
+        qr.push_back({q, p, X, q, nullptr, 0, Rc, p, Tws, 1, nullptr, 0, rk1, n});
         jac.push_back({p, p, Rc, p, nullptr, 0, sig, perm, info, rk1, n});   // rows >= n r' zero
         tr.push_back({sig, perm, p, rank});
         sel.push_back({Rc, p, sig, perm, rank, p, q, p, Vt, p, 1});
@@ -195,10 +196,8 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
     B.copy(cpX);
     B.qr(qr);
     B.qr(qr2);
-    B.copy(cpR);
     B.jacobi(jac);
     B.trunc(tr, tol, rmax);
-    B.zero(zb);
     B.select(sel);
     B.gemm(g2);      // reads U (p >= q) or core j (p < q) before qapply / cpW overwrite them
     B.qapply(qa);
@@ -526,14 +525,17 @@ void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<i
       const double* Wk = W[i][k + 1];                 // r_{k+1} x s, leading dimension r_{k+1}
       double* P = nullptr;                             // Q^T y_k, its q nonzero rows (leading dimension pld)
       long long pld = q;
+      // core k has the layout of an m-row factor with column stride m when its left capacity is
+      // e: a Q is then written there by its QR, not copied
+      const bool in_core = (yc == e[i]);
       if (q == s) {                                    // F
         P = B.wd((size_t)q * c);
         double* Z = B.wd((size_t)m * s);
-        double* Q = B.wd((size_t)m * s);
+        double* Q = in_core ? core : B.wd((size_t)m * s);
         double* Tws = B.wd(qr_tws(m, s));
         gz.push_back(gd(m, s, c, Yk, 1, yld, Wk, 1, c, Z, 1, m, wscale));
         qrZ.push_back({m, s, Z, m, Q, m, nullptr, 0, Tws});
-        cpC.push_back(cd3(Q, core, e[i], n, s, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
+        if (!in_core) cpC.push_back(cd3(Q, core, e[i], n, s, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
         gp.push_back(gd(s, c, m, Q, m, 1, Yk, 1, yld, P, 1, s));
       } else if (q == c && !complete) {                // T, reduced: core k = Q1, Q^T y_k = R1
         double* Yw = const_cast<double*>(Yk);
@@ -541,10 +543,10 @@ void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<i
           Yw = B.wd((size_t)m * c);
           cp0.push_back(cd2(Yk, Yw, m, c, 1, yld, 1, m));
         }
-        double* Q1 = B.wd((size_t)m * c);
+        double* Q1 = in_core ? core : B.wd((size_t)m * c);
         P = B.wd((size_t)c * c);
         qrY.push_back({m, c, Yw, m, Q1, m, P, c, B.wd(qr_tws(m, c))});
-        cpC.push_back(cd3(Q1, core, e[i], n, c, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
+        if (!in_core) cpC.push_back(cd3(Q1, core, e[i], n, c, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
       } else if (q == c) {                             // T: c < m, c < s
         double* Yw = const_cast<double*>(Yk);
         if (k == 0) {                                  // the QR overwrites its input: not x's core
@@ -587,11 +589,11 @@ void emit_rand_sweep(Builder& B, ttc_batch* x, ttc_batch* y, const std::vector<i
       } else {                                         // W: q = m <= c, m < s
         P = B.wd((size_t)q * c);
         double* M1 = B.wd((size_t)m * m);
-        double* QM = B.wd((size_t)m * m);
+        double* QM = in_core ? core : B.wd((size_t)m * m);
         double* TwsM = B.wd(qr_tws(m, m));
         gz.push_back(gd(m, m, c, Yk, 1, yld, Wk, 1, c, M1, 1, m, wscale));
         qrZ.push_back({m, m, M1, m, QM, m, nullptr, 0, TwsM});
-        cpC.push_back(cd3(QM, core, e[i], n, m, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
+        if (!in_core) cpC.push_back(cd3(QM, core, e[i], n, m, 1, e[i], (long long)e[i] * n, 1, yc, (long long)yc * n));
         if (complete) outside_units(cpC, core, e[i], rh, n, yc, m, (long long)rhn - m);
         gp.push_back(gd(m, c, m, QM, m, 1, Yk, 1, yld, P, 1, m));
       }

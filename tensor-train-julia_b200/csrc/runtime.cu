@@ -568,14 +568,15 @@ void Builder::select(const std::vector<SelectDesc>& v) {
   if (v.empty()) return;
   int mr = 0, mc = 0;
   for (auto& d : v) {
-    mr = std::max(mr, d.rows); mc = std::max(mc, d.cols);
+    const int rows = std::max(d.rows, d.zrows);
+    mr = std::max(mr, rows); mc = std::max(mc, d.cols);
     const bool on = wsbase != nullptr;
     chk(on, d.X, (long long)d.ldx * (d.src_cols - 1) + d.rows, 8, "select X");
     chk(on, d.sigma, d.src_cols, 8, "select sigma");
     chk(on, d.perm, d.src_cols, 4, "select perm");
     chk(on, d.rank, 1, 4, "select rank");
-    chk(on, d.U, (long long)d.ldu * (d.cols - 1) + d.rows, 8, "select U");
-    TTC_REQUIRE(d.ldx >= d.rows && d.ldu >= d.rows, TTC_EINTERNAL, "select: leading dims");
+    chk(on, d.U, (long long)d.ldu * (d.cols - 1) + rows, 8, "select U");
+    TTC_REQUIRE(d.ldx >= d.rows && d.ldu >= rows, TTC_EINTERNAL, "select: leading dims");
   }
   Op op; op.kind = OP_SELECT; op.off = plan->push(v); op.count = (int)v.size(); op.a = mr; op.b = mc;
   plan->ops.push_back(op);

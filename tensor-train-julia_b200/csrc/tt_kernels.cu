@@ -166,11 +166,12 @@ void launch_truncate(const TruncDesc* d, int count, double tol, long long rmax, 
 __global__ void select_kernel(const SelectDesc* __restrict__ descs) {
   const SelectDesc D = descs[blockIdx.y];
   const int k = *D.rank;
-  const long long total = (long long)D.rows * D.cols;
+  const int rows = max(D.rows, D.zrows);
+  const long long total = (long long)rows * D.cols;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(e / D.rows), r = (int)(e - (long long)c * D.rows);
+    const int c = (int)(e / rows), r = (int)(e - (long long)c * rows);
     double v = 0.0;
-    if (c < k) {
+    if (c < k && r < D.rows) {
       const int src = D.perm[c];
       v = D.X[(long long)src * D.ldx + r];
       if (D.scale == 1) { const double s = D.sigma[src]; v = (s > 0.0) ? v / s : 0.0; }
