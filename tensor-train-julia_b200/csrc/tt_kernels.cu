@@ -120,37 +120,51 @@ void launch_sumsq(const NormDesc* d, int count, cudaStream_t s) {
 
 // ---------------------------------------------------------------- truncation rule
 // floor(s, tol; degen_tol=1e-5) of src/tt_rounding.jl:297-315 on the sorted values, then
-// k = min(k, rmax, #(s > 0)) (src/tt_rounding.jl:198-199).  One thread per problem: the
-// rule is a short sequential scan in FP64.
-__global__ void truncate_kernel(const TruncDesc* __restrict__ descs, int count, double tol, long long rmax) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+// k = min(k, rmax, #(s > 0)) (src/tt_rounding.jl:198-199).  One warp per problem: the lanes
+// gather the sorted values into shared memory and count the positive ones; lane 0 then runs the
+// rule as a sequential FP64 scan (the sums in the reference's order) over shared memory, eight
+// loads in flight at a time.
+constexpr int kTruncStage = 2048;
+__global__ void __launch_bounds__(32) truncate_kernel(const TruncDesc* __restrict__ descs, int count, double tol,
+                                                      long long rmax) {
+  __shared__ double sv[kTruncStage];
+  const int p = blockIdx.x, lane = threadIdx.x;
   if (p >= count) return;
   const TruncDesc D = descs[p];
   const int d = D.n;
+  const bool staged = d <= kTruncStage;
+  int npos = 0;
+  for (int i = lane; i < d; i += 32) {
+    if (staged) sv[i] = D.sigma[D.perm[i]];
+    npos += (D.sigma[i] > 0.0);
+  }
+  npos = __reduce_add_sync(0xffffffffu, npos);
+  __syncwarp();
+  if (lane != 0) return;
+  auto val = [&](int i) { return staged ? sv[i] : D.sigma[D.perm[i]]; };
   int k;
   if (d <= 0) { k = 0; }
   else if (tol == 0.0) { k = d; }
   else {
     double norm2 = 0.0;
-    for (int i = 0; i < d; ++i) { const double v = D.sigma[D.perm[i]]; norm2 = fma(v, v, norm2); }
+#pragma unroll 8
+    for (int i = 0; i < d; ++i) { const double v = val(i); norm2 = fma(v, v, norm2); }
     int i = d;
     double weight = 0.0;
     const double thr = tol * tol * norm2;
     while (i > 0 && weight < thr) {
-      const double v = D.sigma[D.perm[i - 1]];
+      const double v = val(i - 1);
       weight = fma(v, v, weight);
       --i;
     }
     ++i;
     while (i < d) {
-      const double a = D.sigma[D.perm[i - 1]], b = D.sigma[D.perm[i]];
+      const double a = val(i - 1), b = val(i);
       const double ratio = b / a;
       if (isfinite(ratio) && fabs(1.0 - ratio) <= 1e-5) ++i; else break;
     }
     k = i;
   }
-  int npos = 0;
-  for (int i = 0; i < d; ++i) npos += (D.sigma[i] > 0.0);
   if (k > npos) k = npos;
   if ((long long)k > rmax) k = (int)rmax;
   *D.rank_out = k;
@@ -158,7 +172,7 @@ __global__ void truncate_kernel(const TruncDesc* __restrict__ descs, int count, 
 
 void launch_truncate(const TruncDesc* d, int count, double tol, long long rmax, cudaStream_t s) {
   if (count <= 0) return;
-  truncate_kernel<<<(count + 63) / 64, 64, 0, s>>>(d, count, tol, rmax);
+  truncate_kernel<<<count, 32, 0, s>>>(d, count, tol, rmax);
   TTC_CHECK_LAUNCH();
 }
 
