@@ -660,7 +660,6 @@ void round_rand(ttc_context* c, ttc_batch* x, const std::vector<long long>& rks,
   const int N = x->N;
   TTC_REQUIRE((int)rks.size() == N + 1, TTC_EDIM, "ttrand_rounding: rks must have length N+1");
   TTC_REQUIRE(rks[N] == 1, TTC_EDIM, "ttrand_rounding: rks[N+1] must be 1");
-  TTC_REQUIRE(!o.orthogonal || o.block_rks > 0 || true, TTC_EARG, "");
   batch_sync_ranks(x);
   for (int t = 0; t < x->count; ++t)
     TTC_REQUIRE(x->rk(t, N) == 1, TTC_EDIM, "ttrand_rounding: the last TT rank must be 1");
