@@ -199,7 +199,8 @@ void emit_svd_left(Builder& B, ttc_batch* y, const std::vector<int>& tts, const 
     B.jacobi(jac);
     B.trunc(tr, tol, rmax);
     B.select(sel);
-    B.gemm(g2);      // reads U (p >= q) or core j (p < q) before qapply / cpW overwrite them
+    B.gemm(g2);      // reads U (p >= q) or Cj (p < q; core j itself at the first bond) before
+                     // qapply / cpW overwrite them
     B.qapply(qa);
     B.copy(cpW);
     B.gemm(g3);
